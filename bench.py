@@ -1,0 +1,455 @@
+"""Benchmark: pyheat3d's stencil hot path on B200 (one JSON line on rank 0).
+
+Workload (per rank): the plain GPU path at roofline size — 3D 512^3 fp32, periodic, FTCS heat
+with r = 0.95/6, uniform random [0, 1) field from seed 0, advanced by the single-step TMA
+z-march kernel (``b200/zmarch``). One bench *step* is one solve of ``--time-steps`` updates
+(1000 by default). The metric is GLUPS: site updates (every cell, periodic) per second.
+
+- ``value``: device time of K solves with the field resident in HBM (CUDA events on the launching
+  stream, max over ranks), inputs larger than L2 (512 MiB per field vs 126 MB L2).
+- ``e2e``: the same K solves through the public stepper API with a host->device copy of the
+  initial field from pinned memory before and a device->host copy of the result after each
+  solve inside the timed region.
+- ``roofline``: the z-march kernel's algorithmic bytes (8 B per fp32 update: one read and one
+  write of every value) per launch over its average launch time, against the measured HBM copy
+  bandwidth.
+- ``variants``: the other kernels of the same workload (tb2/3/4/8, 16-bit storage) and the 2D
+  16384^2 fp32 periodic grid (r = 0.95/4), one solve each, for the per-variant roofline figures.
+- ``cpu_baseline``: the NumPy oracle (pyheat3d's reference algorithm restated) on this host, on a
+  bounded sample of the same workload.
+
+``--impl reference`` times the reference's CPU path (the NumPy oracle, thread-chunked over
+z-slabs with every host core) on the same workload and prints the same line with
+``"impl": "reference"``. Multi-GPU (torchrun): every rank advances its own 512^3 field (replicas,
+weak scaling); there is no data-path collective.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N3 = 512
+N2 = 16384
+R3 = 0.95 / 6
+R2 = 0.95 / 4
+FALLBACK_HBM_GBS = 6650.0
+NVSMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def parse() -> argparse.Namespace:
+    ap = argparse.ArgumentParser(description=__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5, help="timed solves")
+    ap.add_argument("--warmup", type=int, default=3, help="untimed solves (>= 3)")
+    ap.add_argument("--time-steps", type=int, default=1000, help="updates per solve")
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--no-variants", action="store_true", help="skip the per-variant table")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------------------------
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def field(n: int, dims: int, seed: int = 0) -> np.ndarray:
+    return np.random.default_rng(seed).random((n,) * dims, dtype=np.float32)
+
+
+class Clocks:
+    """nvidia-smi sampler (200 ms) running while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"ph3_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={NVSMI_FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self) -> dict:
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[4:]))
+            except ValueError:
+                continue
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [r for r in rows if r[2] > 300.0] or rows
+        names = ["active_mask", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = set()
+        for r in load:
+            for nm, v in zip(names[1:], r[3][1:]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r[0] for r in load), "sm_max_mhz": rows[0][1],
+                "samples": len(load), "power_w_max": max(r[2] for r in rows),
+                "reasons": sorted(reasons)}
+
+
+def profile_traffic(name: str) -> float | None:
+    """DRAM bytes per launch from a committed ncu summary (``dram_bytes_per_launch: N`` line)."""
+    p = ROOT / "profiles" / name
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def copy_bandwidth(torch, nbytes: int = 1 << 30, iters: int = 20, repeats: int = 5) -> float:
+    """Device copy_ bandwidth in GB/s, read + write counted, median (pyheat3d roofline.py:8-29)."""
+    n = nbytes // 4
+    a = torch.empty(n, device="cuda", dtype=torch.float32).uniform_()
+    b = torch.empty_like(a)
+    for _ in range(3):
+        b.copy_(a)
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(repeats):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(iters):
+            b.copy_(a)
+        e.record()
+        e.synchronize()
+        out.append(2.0 * 4 * n * iters / (s.elapsed_time(e) * 1e-3) / 1e9)
+    del a, b
+    torch.cuda.empty_cache()
+    return float(np.median(out))
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------------------------
+def dist_init(torch):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def barrier(torch, ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(torch, ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+# the b200 arm
+# ---------------------------------------------------------------------------------------------
+def time_solves(torch, st, nsolves: int, tsteps: int) -> float:
+    """Device seconds of `nsolves` solves on the current stream (field resident)."""
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(nsolves):
+        st.step(tsteps)
+    e.record()
+    e.synchronize()
+    return s.elapsed_time(e) * 1e-3
+
+
+def variant_row(torch, key: str, u0: np.ndarray, stencil, tsteps: int, copy_bw: float) -> dict:
+    from pyheat3d_b200.registry import VARIANTS, make_stepper
+
+    var = VARIANTS[key]
+    st = make_stepper(key, u0, stencil)
+    st.step(max(3 * var.steps_per_pass, 6))
+    torch.cuda.synchronize()
+    secs = time_solves(torch, st, 1, tsteps)
+    ok = bool(np.isfinite(st.get_tensor().float().sum().item()))
+    st.close()
+    cells = u0.size
+    glups = cells * tsteps / secs / 1e9
+    bpu = 2.0 * var.bytes_per_value / var.steps_per_pass
+    return {"glups": round(glups, 2), "bytes_per_update": bpu,
+            "effective_GBs": round(glups * bpu, 1), "frac_copy": round(glups * bpu / copy_bw, 4),
+            "k": var.steps_per_pass, "storage": var.storage, "finite": ok}
+
+
+def cpu_sample(u0: np.ndarray, c0: float, c1: float, threads: int, sweeps: int) -> float:
+    """GLUPS of the NumPy oracle on `sweeps` updates of u0 (periodic) with `threads` workers."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import reference_step, threaded_step
+
+    u = u0.copy()
+    out = np.empty_like(u)
+    if threads == 1:
+        t0 = time.perf_counter()
+        for _ in range(sweeps):
+            u = reference_step(u, c0, c1, "periodic")
+        dt = time.perf_counter() - t0
+    else:
+        with ThreadPoolExecutor(threads) as pool:
+            threaded_step(u, out, c0, c1, "periodic", threads=threads, pool=pool)  # warm
+            t0 = time.perf_counter()
+            for _ in range(sweeps):
+                threaded_step(u, out, c0, c1, "periodic", threads=threads, pool=pool)
+                u, out = out, u
+            dt = time.perf_counter() - t0
+    return u0.size * sweeps / dt / 1e9
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_b200(a: argparse.Namespace) -> None:
+    import torch
+
+    from pyheat3d_b200 import _lib, heat_stencil
+    from pyheat3d_b200.registry import make_stepper
+
+    ws, rank, local = dist_init(torch)
+    T, K, W = a.time_steps, a.steps, max(3, a.warmup)
+    hbm_peak, peak_kind = peaks()
+    copy_bw = copy_bandwidth(torch)
+    stencil = heat_stencil(3, R3, "periodic")
+    u0 = field(N3, 3, seed=rank)
+    cells = u0.size
+
+    # ---- value: K solves, field resident in HBM
+    st = make_stepper("b200/zmarch", u0, stencil)
+    for _ in range(W):
+        st.step(T)
+    barrier(torch, ws)
+    with Clocks(local) as clk:
+        secs = time_solves(torch, st, K, T)
+    barrier(torch, ws)
+    secs = max_over_ranks(torch, ws, secs)
+    clocks = clk.summary()
+    launches = K * T
+    value = ws * cells * T * K / secs / 1e9
+    launch_s = secs / launches
+    alg_bytes = 8.0 * cells  # one fp32 read + one fp32 write per site update
+    achieved = alg_bytes / launch_s / 1e9
+    final_ok = bool(np.isfinite(st.get_tensor().sum().item()))
+
+    # ---- e2e: pinned H2D of the initial field, K solves through the stepper API, D2H result
+    pin_in = torch.from_numpy(u0).pin_memory()
+    pin_out = torch.empty(u0.shape, dtype=torch.float32).pin_memory()
+    st.set_state(pin_in)
+    st.step(T)
+    st.get(out=pin_out)
+    barrier(torch, ws)
+    t0 = time.perf_counter()
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s_ev.record()
+    for _ in range(K):
+        st.set_state(pin_in)
+        st.step(T)
+        st.get(out=pin_out)
+    e_ev.record()
+    e_ev.synchronize()
+    e2e_secs = max(s_ev.elapsed_time(e_ev) * 1e-3, 0.0)
+    wall = time.perf_counter() - t0
+    e2e_secs = max_over_ranks(torch, ws, max(e2e_secs, wall))
+    st.close()
+    del st
+    torch.cuda.empty_cache()
+    if _lib.device_status(clear=True) != 0:
+        raise RuntimeError("kernel status word set during the bench")
+
+    # ---- per-variant table (rank 0 of a 1-GPU run)
+    variants = {}
+    if ws == 1 and not a.no_variants:
+        for key in ("b200/naive", "b200/tb2", "b200/tb3", "b200/tb4", "b200/tb8",
+                    "b200/zmarch-bf16", "b200/tb4-bf16", "b200/zmarch-fp16"):
+            try:
+                variants["3d512_" + key.split("/")[1]] = variant_row(torch, key, u0, stencil, T,
+                                                                     copy_bw)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                variants["3d512_" + key.split("/")[1]] = {"error": str(e)[:200]}
+        u2 = field(N2, 2)
+        st2 = heat_stencil(2, R2, "periodic")
+        for key in ("b200/ymarch", "b200/naive", "b200/tb2", "b200/tb4", "b200/tb8",
+                    "b200/ymarch-bf16", "b200/tb4-fp16"):
+            try:
+                variants["2d16384_" + key.split("/")[1]] = variant_row(torch, key, u2, st2, T,
+                                                                       copy_bw)
+            except Exception as e:  # pragma: no cover
+                variants["2d16384_" + key.split("/")[1]] = {"error": str(e)[:200]}
+        del u2
+
+    # ---- CPU baseline (rank 0, N = 1)
+    cpu = None
+    if ws == 1 and rank == 0 and not a.no_cpu:
+        cores = host_cores()
+        one = cpu_sample(u0, stencil.c0, stencil.c1, 1, 4)
+        allc = cpu_sample(u0, stencil.c0, stencil.c1, cores, 12)
+        cpu = {"value": round(allc, 4), "unit": "GLUPS", "cores": cores, "kind": "port",
+               "sample": f"NumPy oracle, 12 periodic updates of the same 512^3 fp32 field, "
+                         f"thread-chunked over z-slabs ({cores} threads)",
+               "value_1core": round(one, 4),
+               "sample_1core": "NumPy oracle, 4 updates of the 512^3 field, 1 thread "
+                               "(pyheat3d numpy/slicing)"}
+
+    if rank == 0:
+        traffic = profile_traffic("zmarch_tma_512cubed_fp32.md")
+        line = {
+            "metric": "GLUPS (3D 512^3 fp32 periodic FTCS, single-step TMA z-march)",
+            "value": round(value, 2), "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
+            "ms_per_step": round(secs / K * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "3D 512^3 fp32 periodic heat, r=0.95/6, uniform[0,1) seed 0 "
+                                   "(rank r: seed r), b200/zmarch",
+                       "grid": [N3, N3, N3], "bc": "periodic", "storage": "float32",
+                       "time_steps_per_step": T, "units": "site updates (all cells)",
+                       "l2": "inputs larger than L2 (512 MiB field vs 126 MB L2)",
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+                         "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "copy_bw_same_run": round(copy_bw, 1),
+                         "frac_of_copy_same_run": round(achieved / copy_bw, 4),
+                         "alg_bytes_per_launch": alg_bytes,
+                         "launch_ms": round(launch_s * 1e3, 5)},
+            "e2e": {"value": round(ws * cells * T * K / e2e_secs / 1e9, 2), "unit": "GLUPS",
+                    "h2d_bytes_per_step": int(u0.nbytes), "d2h_bytes_per_step": int(u0.nbytes)},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "variants": variants,
+            "finite": final_ok,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------
+# the reference arm: the reference's CPU path (NumPy oracle), all host threads
+# ---------------------------------------------------------------------------------------------
+def run_reference(a: argparse.Namespace) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import threaded_step
+
+    cores = host_cores()
+    u = field(N3, 3)
+    out = np.empty_like(u)
+    c0, c1 = np.float32(1.0 - 6.0 * R3), np.float32(R3)
+    sweeps = 1  # one update of the 512^3 field per bench step (bounded sample of a solve)
+    W, K = max(3, a.warmup), a.steps
+    with ThreadPoolExecutor(cores) as pool:
+        for _ in range(W):
+            threaded_step(u, out, c0, c1, "periodic", threads=cores, pool=pool)
+            u, out = out, u
+        t0 = time.perf_counter()
+        for _ in range(K * sweeps):
+            threaded_step(u, out, c0, c1, "periodic", threads=cores, pool=pool)
+            u, out = out, u
+        secs = time.perf_counter() - t0
+    value = u.size * sweeps * K / secs / 1e9
+    line = {
+        "impl": "reference",
+        "metric": "GLUPS (3D 512^3 fp32 periodic FTCS, single-step TMA z-march)",
+        "value": round(value, 4), "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
+        "ms_per_step": round(secs / K * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "3D 512^3 fp32 periodic heat, r=0.95/6, uniform[0,1) seed 0",
+                   "grid": [N3, N3, N3], "bc": "periodic", "storage": "float32",
+                   "time_steps_per_step": sweeps, "units": "site updates (all cells)"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GLUPS", "cores": cores,
+                         "kind": "port",
+                         "sample": f"{sweeps} update of the 512^3 field per step, NumPy oracle "
+                                   f"(pyheat3d reference_step restated) chunked over z-slabs on "
+                                   f"{cores} threads"},
+        "e2e": {"value": round(value, 4), "unit": "GLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)

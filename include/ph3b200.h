@@ -1,0 +1,117 @@
+/*
+ * ph3b200.h — C ABI of the pyheat3d B200 stencil backend (libph3b200.so, sm_100a).
+ *
+ * Conventions
+ * - The caller owns all memory: every pointer is a device pointer the caller allocated
+ *   (cudaMalloc, torch, ...). Entry points allocate nothing on the device.
+ * - Arrays are C-ordered (z, y, x) in 3D and (y, x) in 2D with x contiguous. Storage is fp32,
+ *   fp16 or bf16 (PH3_FLOAT32 / PH3_FLOAT16 / PH3_BFLOAT16); arithmetic is always fp32 and every
+ *   result is bit-identical to pyheat3d's NumPy reference in the canonical summation order.
+ * - `src` (optional, may be NULL) is the additive Jacobi source b, fp32, same shape as u.
+ * - `u` and `out` must not alias (ping-pong). With PH3_DIRICHLET the outer layer of `out` is
+ *   never written, so both buffers must carry the same boundary values.
+ * - `stream` is a cudaStream_t (NULL = legacy default stream). Launches are asynchronous; no
+ *   entry point synchronises the device unless its comment says so.
+ * - Every function returns PH3_OK (0) or an error code; ph3_last_error() then gives a message
+ *   (thread-local). Entry points are re-entrant.
+ *
+ * Reference interfaces replaced (pyheat3d, paths relative to the project root):
+ *   src/pyheat3d/backends/stencil.cu        the NVRTC kernels naive2d/naive3d/zmarch3d/tb3d/tb2d
+ *   src/pyheat3d/backends/cupy_backend.py   CupyStepper._launch / step (launch + remainder rule)
+ */
+#ifndef PH3B200_H
+#define PH3B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* return codes */
+#define PH3_OK 0
+#define PH3_EINVAL 1       /* invalid argument (shape, pointer, storage, k, ...) */
+#define PH3_ECUDA 2        /* a CUDA runtime call failed (message has the CUDA error string) */
+#define PH3_EUNSUPPORTED 3 /* valid request this build cannot serve (e.g. grid too large) */
+#define PH3_EDEVICE 4      /* a kernel reported an expired bounded wait (see ph3_device_status) */
+
+/* storage types (stencil.cu:16-30 STORAGE macro: 0 fp32, 1 fp16, 2 bf16) */
+#define PH3_FLOAT32 0
+#define PH3_FLOAT16 1
+#define PH3_BFLOAT16 2
+
+/* boundary conditions (problem.py:18-21; stencil.cu PERIODIC macro) */
+#define PH3_DIRICHLET 0
+#define PH3_PERIODIC 1
+
+/* kernel families for ph3_advance */
+#define PH3_VARIANT_NAIVE 0 /* one site per thread (stencil.cu:43-93) */
+#define PH3_VARIANT_MARCH 1 /* single-step march: TMA z-march in 3D, y-march in 2D */
+#define PH3_VARIANT_TB 2    /* temporal blocking, k fused steps per pass */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int ph3_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* ph3_last_error(void);
+
+/* Number of SMs of the current device (0 and an error message if no device). */
+int ph3_sm_count(void);
+
+/*
+ * Read the current device's kernel status word into *code (0 = no expired wait) and reset it
+ * when `clear` is nonzero. Synchronises the current device.
+ */
+int ph3_device_status(int* code, int clear);
+
+/*
+ * One update, one site per thread.
+ * Replaces stencil.cu:43-64 naive2d(u, o, ny, nx, c0, c1) / :66-93 naive3d(u, o, nz, ny, nx,
+ * c0, c1), where STORAGE and PERIODIC were NVRTC macros; here they are arguments.
+ */
+int ph3_naive2d(const void* u, void* out, const float* src, int ny, int nx, float c0, float c1,
+                int storage, int bc, void* stream);
+int ph3_naive3d(const void* u, void* out, const float* src, int nz, int ny, int nx, float c0,
+                float c1, int storage, int bc, void* stream);
+
+/*
+ * One update by the 3D z-march. Replaces stencil.cu:101-161 zmarch3d(u, o, nz, ny, nx, c0, c1)
+ * (BX/BY/ZCH macros -> `chunk`, the z-planes per work item; <= 0 picks a default). Uses TMA
+ * plane staging when nx*sizeof(storage) is a multiple of 16 bytes and the buffers are 16-byte
+ * aligned, otherwise a plain-load register march; the results are identical.
+ */
+int ph3_zmarch3d(const void* u, void* out, const float* src, int nz, int ny, int nx, float c0,
+                 float c1, int storage, int bc, int chunk, void* stream);
+
+/*
+ * One update by the 2D y-march. Replaces stencil.cu:289-385 tb2d with K = 1 ("ymarch",
+ * cupy_backend.py:63-70). `chunk` = rows per block (<= 0: default).
+ */
+int ph3_ymarch2d(const void* u, void* out, const float* src, int ny, int nx, float c0, float c1,
+                 int storage, int bc, int chunk, void* stream);
+
+/*
+ * k fused updates in one pass (temporal blocking), k in {2, 3, 4, 8}; intermediate levels stay
+ * in fp32 and are rounded to storage once per pass. Replaces stencil.cu:178-281
+ * tb3d(u, o, nz, ny, nx, c0, c1) and :289-385 tb2d(u, o, ny, nx, c0, c1) (K macro -> k).
+ */
+int ph3_tb3d(const void* u, void* out, const float* src, int nz, int ny, int nx, int k, float c0,
+             float c1, int storage, int bc, int chunk, void* stream);
+int ph3_tb2d(const void* u, void* out, const float* src, int ny, int nx, int k, float c0,
+             float c1, int storage, int bc, int chunk, void* stream);
+
+/*
+ * Advance `nsteps` time steps / Jacobi sweeps on the ping-pong pair (a, b), starting from the
+ * state in `a`: nsteps / k passes of the variant's main kernel, then nsteps % k single steps
+ * (cupy_backend.py:188-194). *in_b is set to 1 when the final state is in `b`, else 0.
+ * nz must be 1 when dims == 2. k must be 1 for the naive and march variants.
+ */
+int ph3_advance(int dims, int nz, int ny, int nx, int storage, int bc, float c0, float c1,
+                int variant, int k, void* a, void* b, const float* src, int64_t nsteps,
+                void* stream, int* in_b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PH3B200_H */

@@ -1,0 +1,190 @@
+// Shared device helpers of the pyheat3d B200 stencil kernels (sm_100a).
+//
+// The update every kernel computes (pyheat3d src/pyheat3d/problem.py:3-10,
+// src/pyheat3d/backends/numpy_ref.py:30-47):
+//
+//     u'[c] = c0*u[c] + c1*S[c]  (+ b[c], added last)
+//     S     = ((u[x-1]+u[x+1]) + (u[y-1]+u[y+1])) + (u[z-1]+u[z+1])
+//
+// Arithmetic is fp32 for every storage type. Every add and multiply is an explicitly rounded
+// __fadd_rn / __fmul_rn so nvcc cannot contract c0*u + c1*S into an FMA: the result is then
+// bit-identical to NumPy, which rounds each ufunc separately.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ph3 {
+
+// ------------------------------------------------------------------------------------------
+// storage traits: load converts to fp32 exactly, store rounds to nearest even
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float to_f(float v) { return v; }
+__device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
+__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+template <typename T> __device__ __forceinline__ T from_f(float v);
+template <> __device__ __forceinline__ float from_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float v) {
+    return __float2bfloat16_rn(v);
+}
+
+template <typename T> __device__ __forceinline__ float ldg1(const T* p) { return to_f(__ldg(p)); }
+
+// Vector of V storage elements moved as one 4/8/16-byte access.
+template <typename T, int V> struct VecBits;
+template <typename T> struct VecBits<T, 1> { using type = T; };
+template <int V> struct VecBytes;
+template <> struct VecBytes<4> { using type = uint32_t; };
+template <> struct VecBytes<8> { using type = uint2; };
+template <> struct VecBytes<16> { using type = uint4; };
+
+template <typename T, int V>
+__device__ __forceinline__ void ld_vec(const T* __restrict__ p, float (&v)[V]) {
+    constexpr int B = int(sizeof(T)) * V;
+    if constexpr (B == 2) {
+        v[0] = to_f(__ldg(p));
+    } else {
+        using W = typename VecBytes<B>::type;
+        union { W w; T e[V]; } u;
+        u.w = __ldg(reinterpret_cast<const W*>(p));
+#pragma unroll
+        for (int j = 0; j < V; ++j) v[j] = to_f(u.e[j]);
+    }
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void st_vec(T* __restrict__ p, const float (&v)[V]) {
+    constexpr int B = int(sizeof(T)) * V;
+    if constexpr (B == 2) {
+        *p = from_f<T>(v[0]);
+    } else {
+        using W = typename VecBytes<B>::type;
+        union { W w; T e[V]; } u;
+#pragma unroll
+        for (int j = 0; j < V; ++j) u.e[j] = from_f<T>(v[j]);
+        *reinterpret_cast<W*>(p) = u.w;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// canonical-order stencil arithmetic
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float upd2(float c0, float c1, float ctr, float xm, float xp,
+                                      float ym, float yp) {
+    const float s = __fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym, yp));
+    return __fadd_rn(__fmul_rn(c0, ctr), __fmul_rn(c1, s));
+}
+
+__device__ __forceinline__ float upd3(float c0, float c1, float ctr, float xm, float xp,
+                                      float ym, float yp, float zm, float zp) {
+    const float s = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym, yp)), __fadd_rn(zm, zp));
+    return __fadd_rn(__fmul_rn(c0, ctr), __fmul_rn(c1, s));
+}
+
+__device__ __forceinline__ int wrap_idx(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+__device__ __forceinline__ int clamp_idx(int i, int lo, int hi) {
+    return i < lo ? lo : (i > hi ? hi : i);
+}
+
+// ------------------------------------------------------------------------------------------
+// error word: kernels whose bounded waits expire record a code here and return early
+// ------------------------------------------------------------------------------------------
+enum DeviceError : int {
+    kDevOk = 0,
+    kDevMbarTimeout = 1,     // an mbarrier wait hit its iteration limit
+    kDevDependTimeout = 2,   // a persistent work item waited too long for its predecessors
+    kDevStopRequested = 3,   // a persistent kernel saw the host stop word
+};
+// `err` points at the per-device status word owned by the C-ABI layer (may be null).
+__device__ __forceinline__ void record_error(int* err, int code) {
+    if (err != nullptr) atomicCAS(err, 0, code);
+}
+
+// Iteration limit of every spin-wait (each iteration also backs off with __nanosleep), giving
+// well over a second of waiting before a wait is declared stuck.
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// ------------------------------------------------------------------------------------------
+// mbarrier + TMA (cp.async.bulk) wrappers, written from the PTX ISA
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase. Returns false (and records the error) on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+    if (mbar_try_wait(bar, parity)) return true;
+    for (uint32_t it = 0; it < kSpinLimit; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (it > 64) __nanosleep(it > 4096 ? 256 : 32);
+    }
+    record_error(err, kDevMbarTimeout);
+    return false;
+}
+
+// 3D tiled tensor load global -> shared, completion counted on an mbarrier (bytes).
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, int y, int z,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const void* tmap) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
+}
+
+}  // namespace ph3

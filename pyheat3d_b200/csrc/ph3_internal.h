@@ -1,0 +1,41 @@
+// Host-side declarations shared by the kernel translation units and the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ph3 {
+
+enum Storage : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
+
+// One stencil launch: out = step^k(u) for a ping-pong pair (u and out never alias).
+struct Launch {
+    const void* u;
+    void* out;
+    const float* src;   // optional Jacobi source b (fp32, same shape), nullptr if none
+    int dims;           // 2 or 3
+    int nz, ny, nx;     // nz == 1 in 2D
+    bool periodic;
+    int storage;        // Storage
+    float c0, c1;
+    int k;              // fused time steps (1 for single-step kernels)
+    int chunk;          // march chunk length (planes in 3D, rows in 2D); <= 0 picks a default
+    cudaStream_t stream;
+    int* err;           // device status word for bounded waits (may be null)
+};
+
+// Kernel families (ph3_stencil.cu, ph3_zmarch.cu). Each returns the launch status.
+cudaError_t launch_naive(const Launch& L);
+cudaError_t launch_march_k1(const Launch& L);   // register march, k = 1, any shape
+cudaError_t launch_tb(const Launch& L);         // temporal blocking, k in {2,3,4,8}
+cudaError_t launch_zmarch_tma(const Launch& L); // 3D TMA z-march, k = 1, aligned shapes
+bool zmarch_tma_supported(const Launch& L);
+
+// Number of streaming multiprocessors of the current device (cached per device).
+int sm_count();
+
+// Default march chunk: split the marching axis so that at least `target_ctas` blocks exist,
+// never shorter than `min_len` planes; the result is clamped to [1, n_march].
+int default_chunk(int n_march, long long tiles, int min_len, long long target_ctas);
+
+}  // namespace ph3

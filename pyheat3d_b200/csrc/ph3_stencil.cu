@@ -1,0 +1,718 @@
+// Stencil kernels for any grid shape (sm_100a): naive single-site kernels, register marches
+// for one time step, and temporal-blocking (tb<k>) wavefront kernels.
+//
+// Functional spec (what, not how): pyheat3d src/pyheat3d/backends/stencil.cu
+//   naive2d/naive3d :43-93, zmarch3d :101-161, tb3d :178-281, tb2d (K=1 -> ymarch) :289-385,
+// with the launch/remainder semantics of src/pyheat3d/backends/cupy_backend.py:141-194.
+//
+// Layout: C order, (z, y, x) / (y, x), x contiguous; storage fp32, fp16 or bf16; fp32 math.
+// Dirichlet: the outer layer is never written. Periodic: every cell, wrap-around neighbours.
+#include <algorithm>
+
+#include "ph3_common.cuh"
+#include "ph3_internal.h"
+
+namespace ph3 {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ------------------------------------------------------------------------------------------
+// small helpers
+// ------------------------------------------------------------------------------------------
+
+// V fp32 source values starting at p (p aligned to V*4 bytes when vec).
+template <int V>
+__device__ __forceinline__ void ld_src(const float* __restrict__ p, bool vec, float (&v)[V]) {
+    if (vec) {
+        if constexpr (V % 4 == 0) {
+#pragma unroll
+            for (int q = 0; q < V / 4; ++q) {
+                const float4 t = __ldg(reinterpret_cast<const float4*>(p) + q);
+                v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+            }
+        } else if constexpr (V == 2) {
+            const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+            v[0] = t.x; v[1] = t.y;
+        } else {
+            v[0] = __ldg(p);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < V; ++j) v[j] = __ldg(p + j);
+    }
+}
+
+template <bool PER>
+__device__ __forceinline__ int fix_idx(int i, int n) {
+    if constexpr (PER) return wrap_idx(i, n);
+    else return clamp_idx(i, 0, n - 1);
+}
+
+// Column addressing of one thread's V consecutive x-values starting at gx.
+// vec: the V values are one aligned vector (nx % V == 0 and gx % V == 0), addressed by `base`.
+// scalar: each value has its own wrapped / clamped column in cx[].
+template <bool PER, int V>
+struct Cols {
+    int base;
+    int cx[V];
+    __device__ __forceinline__ void init(int gx, int nx, bool vec) {
+        if (vec) {
+            base = PER ? wrap_idx(gx, nx) : clamp_idx(gx, 0, nx - V);
+#pragma unroll
+            for (int j = 0; j < V; ++j) cx[j] = base + j;
+        } else {
+            base = 0;
+#pragma unroll
+            for (int j = 0; j < V; ++j) cx[j] = fix_idx<PER>(gx + j, nx);
+        }
+    }
+    template <typename T>
+    __device__ __forceinline__ void load(const T* __restrict__ row, bool vec, float (&v)[V]) const {
+        if (vec) {
+            ld_vec<T, V>(row + base, v);
+        } else {
+#pragma unroll
+            for (int j = 0; j < V; ++j) v[j] = ldg1(row + cx[j]);
+        }
+    }
+    __device__ __forceinline__ void load_src(const float* __restrict__ row, bool vec,
+                                             float (&v)[V]) const {
+        if (vec) {
+            ld_src<V>(row + base, true, v);
+        } else {
+#pragma unroll
+            for (int j = 0; j < V; ++j) v[j] = __ldg(row + cx[j]);
+        }
+    }
+};
+
+// Store V values at columns gx..gx+V-1 of `row` (unwrapped; only in-domain columns written).
+// `skip` has bit j set for columns that must not be written (Dirichlet boundary).
+template <typename T, int V>
+__device__ __forceinline__ void store_cols(T* __restrict__ row, int gx, int nx, bool vec,
+                                           uint32_t skip, const float (&v)[V]) {
+    if (vec && skip == 0 && gx + V <= nx) {
+        st_vec<T, V>(row + gx, v);
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+        if (gx + j < nx && !((skip >> j) & 1u)) row[gx + j] = from_f<T>(v[j]);
+}
+
+// ------------------------------------------------------------------------------------------
+// naive: one lattice site per thread; every operand through L1/L2
+// ------------------------------------------------------------------------------------------
+template <typename T, bool PER>
+__global__ void __launch_bounds__(256)
+naive2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int ny,
+               int nx, float c0, float c1) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= nx || j >= ny) return;
+    int im, ip, jm, jp;
+    if constexpr (PER) {
+        im = i == 0 ? nx - 1 : i - 1; ip = i == nx - 1 ? 0 : i + 1;
+        jm = j == 0 ? ny - 1 : j - 1; jp = j == ny - 1 ? 0 : j + 1;
+    } else {
+        if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1) return;
+        im = i - 1; ip = i + 1; jm = j - 1; jp = j + 1;
+    }
+    const int64_t r = int64_t(j) * nx;
+    float v = upd2(c0, c1, ldg1(u + r + i), ldg1(u + r + im), ldg1(u + r + ip),
+                   ldg1(u + int64_t(jm) * nx + i), ldg1(u + int64_t(jp) * nx + i));
+    if (b != nullptr) v = __fadd_rn(v, __ldg(b + r + i));
+    o[r + i] = from_f<T>(v);
+}
+
+template <typename T, bool PER>
+__global__ void __launch_bounds__(256)
+naive3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
+               int ny, int nx, float c0, float c1) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= nx || j >= ny || k >= nz) return;
+    int im, ip, jm, jp, km, kp;
+    if constexpr (PER) {
+        im = i == 0 ? nx - 1 : i - 1; ip = i == nx - 1 ? 0 : i + 1;
+        jm = j == 0 ? ny - 1 : j - 1; jp = j == ny - 1 ? 0 : j + 1;
+        km = k == 0 ? nz - 1 : k - 1; kp = k == nz - 1 ? 0 : k + 1;
+    } else {
+        if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1 || k == 0 || k == nz - 1) return;
+        im = i - 1; ip = i + 1; jm = j - 1; jp = j + 1; km = k - 1; kp = k + 1;
+    }
+    const int64_t P = int64_t(nx) * ny;
+    const int64_t c = int64_t(k) * P + int64_t(j) * nx;
+    float v = upd3(c0, c1, ldg1(u + c + i), ldg1(u + c + im), ldg1(u + c + ip),
+                   ldg1(u + int64_t(k) * P + int64_t(jm) * nx + i),
+                   ldg1(u + int64_t(k) * P + int64_t(jp) * nx + i),
+                   ldg1(u + int64_t(km) * P + int64_t(j) * nx + i),
+                   ldg1(u + int64_t(kp) * P + int64_t(j) * nx + i));
+    if (b != nullptr) v = __fadd_rn(v, __ldg(b + c + i));
+    o[c + i] = from_f<T>(v);
+}
+
+// ------------------------------------------------------------------------------------------
+// 2D single step, y-march: warp w of the block owns a strip of 32*V columns (lane l holds
+// columns x0 + l*V .. +V-1 as one vector) and walks a chunk of rows, RB rows per iteration, with
+// the next RB rows already in flight. x-neighbours come from warp shuffles (lanes 0 and 31 load
+// the strip's halo columns), y-neighbours from the row window in registers. No shared memory.
+// ------------------------------------------------------------------------------------------
+template <typename T, bool PER, int V, int W, int RB>
+__global__ void __launch_bounds__(32 * W)
+march2d_k1_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b,
+                  int ny, int nx, float c0, float c1, int ych, int vec_i) {
+    constexpr int EX = 32 * V;
+    const bool vec = vec_i != 0;
+    const int lane = threadIdx.x & 31;
+    const int strip = blockIdx.x * W + (threadIdx.x >> 5);
+    const int x0 = strip * EX;
+    if (x0 >= nx) return;  // whole warp leaves together; no block-wide sync in this kernel
+    const int gx = x0 + lane * V;
+    int ylo = blockIdx.y * ych, yhi = min(ylo + ych, ny);
+    if constexpr (!PER) { ylo = max(ylo, 1); yhi = min(yhi, ny - 1); }
+    if (ylo >= yhi) return;
+
+    Cols<PER, V> cols;
+    cols.init(gx, nx, vec);
+    const int xl = fix_idx<PER>(x0 - 1, nx);
+    const int xr = fix_idx<PER>(x0 + EX, nx);
+    uint32_t skip = 0;  // Dirichlet boundary / outside columns are never written
+    if constexpr (!PER) {
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+            if (gx + j <= 0 || gx + j >= nx - 1) skip |= 1u << j;
+    }
+
+    // window rows ylo-1 .. ylo+RB (RB + 2 rows), halos per row, prefetch RB rows
+    float win[RB + 2][V], hl[RB + 2], hr[RB + 2];
+    float pre[RB][V], pl[RB], pr[RB];
+    auto load_row = [&](int y, float (&v)[V], float& l, float& r) {
+        const T* row = u + int64_t(fix_idx<PER>(y, ny)) * nx;
+        cols.load(row, vec, v);
+        l = lane == 0 ? ldg1(row + xl) : 0.f;
+        r = lane == 31 ? ldg1(row + xr) : 0.f;
+    };
+#pragma unroll
+    for (int q = 0; q < RB + 2; ++q) load_row(ylo - 1 + q, win[q], hl[q], hr[q]);
+
+    for (int y = ylo; y < yhi; y += RB) {
+        const bool more = y + RB < yhi;
+        if (more) {
+#pragma unroll
+            for (int q = 0; q < RB; ++q) load_row(y + RB + 1 + q, pre[q], pl[q], pr[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < RB; ++q) {
+            const int yy = y + q;
+            if (yy >= yhi) break;
+            float out[V];
+            const float left = __shfl_up_sync(kFull, win[q + 1][V - 1], 1);
+            const float right = __shfl_down_sync(kFull, win[q + 1][0], 1);
+            float bv[V];
+            if (b != nullptr) cols.load_src(b + int64_t(yy) * nx, vec, bv);
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                const float xm = j > 0 ? win[q + 1][j - 1] : (lane == 0 ? hl[q + 1] : left);
+                const float xp = j < V - 1 ? win[q + 1][j + 1] : (lane == 31 ? hr[q + 1] : right);
+                float v = upd2(c0, c1, win[q + 1][j], xm, xp, win[q][j], win[q + 2][j]);
+                if (b != nullptr) v = __fadd_rn(v, bv[j]);
+                out[j] = v;
+            }
+            store_cols<T, V>(o + int64_t(yy) * nx, gx, nx, vec, skip, out);
+        }
+        if (more) {
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                win[0][j] = win[RB][j];
+                win[1][j] = win[RB + 1][j];
+            }
+            hl[0] = hl[RB]; hl[1] = hl[RB + 1]; hr[0] = hr[RB]; hr[1] = hr[RB + 1];
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+#pragma unroll
+                for (int j = 0; j < V; ++j) win[q + 2][j] = pre[q][j];
+                hl[q + 2] = pl[q];
+                hr[q + 2] = pr[q];
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// 3D single step, z-march with plain loads (any shape): the block owns an xy tile of 32*V x
+// W*R sites; warp w holds R rows, lane l holds V columns per row as one vector. The z-neighbours
+// form a register queue (below / centre / above) and the plane after `above` is in flight while
+// a plane is computed. x-neighbours: shuffles (+ halo columns loaded by lanes 0 and 31);
+// y-neighbours: own registers, the first/last rows of the neighbouring warps through shared
+// memory, and the tile's halo rows loaded by the first and last warp.
+// ------------------------------------------------------------------------------------------
+template <typename T, bool PER, int V, int R, int W>
+__global__ void __launch_bounds__(32 * W)
+march3d_k1_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b,
+                  int nz, int ny, int nx, float c0, float c1, int zch, int vec_i) {
+    constexpr int EX = 32 * V, EY = W * R;
+    __shared__ __align__(16) float edge[2][W][EX];  // [first/last row][warp][column]
+    const bool vec = vec_i != 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int x0 = blockIdx.x * EX, y0 = blockIdx.y * EY;
+    const int gx = x0 + lane * V, gy0 = y0 + w * R;
+    int zlo = blockIdx.z * zch, zhi = min(zlo + zch, nz);
+    if constexpr (!PER) { zlo = max(zlo, 1); zhi = min(zhi, nz - 1); }
+    if (zlo >= zhi) return;  // uniform over the block
+
+    const int64_t P = int64_t(nx) * ny;
+    Cols<PER, V> cols;
+    cols.init(gx, nx, vec);
+    int64_t roff[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) roff[r] = int64_t(fix_idx<PER>(gy0 + r, ny)) * nx;
+    const int64_t rtop = int64_t(fix_idx<PER>(y0 - 1, ny)) * nx;
+    const int64_t rbot = int64_t(fix_idx<PER>(y0 + EY, ny)) * nx;
+    const int xl = fix_idx<PER>(x0 - 1, nx), xr = fix_idx<PER>(x0 + EX, nx);
+    uint32_t skipx = 0, skipy = 0;
+    if constexpr (!PER) {
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+            if (gx + j <= 0 || gx + j >= nx - 1) skipx |= 1u << j;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (gy0 + r <= 0 || gy0 + r >= ny - 1) skipy |= 1u << r;
+    }
+
+    struct Plane {
+        float v[R][V];
+        float l[R], r[R];    // halo columns (lanes 0 / 31)
+        float t[V], bt[V];   // halo rows (warp 0 / warp W-1)
+    };
+    auto load_plane = [&](int z, Plane& p) {
+        const T* pl = u + int64_t(fix_idx<PER>(z, nz)) * P;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            cols.load(pl + roff[r], vec, p.v[r]);
+            p.l[r] = lane == 0 ? ldg1(pl + roff[r] + xl) : 0.f;
+            p.r[r] = lane == 31 ? ldg1(pl + roff[r] + xr) : 0.f;
+        }
+        if (w == 0) cols.load(pl + rtop, vec, p.t);
+        if (w == W - 1) cols.load(pl + rbot, vec, p.bt);
+    };
+
+    float bel[R][V];
+    Plane ctr, abv, pre;
+    {
+        const T* pl = u + int64_t(fix_idx<PER>(zlo - 1, nz)) * P;
+#pragma unroll
+        for (int r = 0; r < R; ++r) cols.load(pl + roff[r], vec, bel[r]);
+    }
+    load_plane(zlo, ctr);
+    load_plane(zlo + 1, abv);
+
+    for (int z = zlo; z < zhi; ++z) {
+        const bool more = z + 1 < zhi;
+        if (more) load_plane(z + 2, pre);
+        // y-neighbours across warps
+        float up[V], dn[V];
+        if constexpr (W > 1) {
+            __syncthreads();  // previous iteration's reads of edge[] are done
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                edge[0][w][lane * V + j] = ctr.v[0][j];
+                edge[1][w][lane * V + j] = ctr.v[R - 1][j];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                up[j] = w > 0 ? edge[1][w - 1][lane * V + j] : ctr.t[j];
+                dn[j] = w < W - 1 ? edge[0][w + 1][lane * V + j] : ctr.bt[j];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < V; ++j) { up[j] = ctr.t[j]; dn[j] = ctr.bt[j]; }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float left = __shfl_up_sync(kFull, ctr.v[r][V - 1], 1);
+            const float right = __shfl_down_sync(kFull, ctr.v[r][0], 1);
+            float bv[V];
+            if (b != nullptr) cols.load_src(b + int64_t(z) * P + roff[r], vec, bv);
+            float out[V];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                const float xm = j > 0 ? ctr.v[r][j - 1] : (lane == 0 ? ctr.l[r] : left);
+                const float xp = j < V - 1 ? ctr.v[r][j + 1] : (lane == 31 ? ctr.r[r] : right);
+                const float ym = r > 0 ? ctr.v[r - 1][j] : up[j];
+                const float yp = r < R - 1 ? ctr.v[r + 1][j] : dn[j];
+                float v = upd3(c0, c1, ctr.v[r][j], xm, xp, ym, yp, bel[r][j], abv.v[r][j]);
+                if (b != nullptr) v = __fadd_rn(v, bv[j]);
+                out[j] = v;
+            }
+            const int gy = gy0 + r;
+            if (gy < ny && !((skipy >> r) & 1u))
+                store_cols<T, V>(o + int64_t(z) * P + int64_t(gy) * nx, gx, nx, vec, skipx, out);
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int j = 0; j < V; ++j) bel[r][j] = ctr.v[r][j];
+        ctr = abv;
+        if (more) abv = pre;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// temporal blocking, 3D: k fused steps per pass, (z, t) wavefront with overlapped tiling.
+// The block's extended xy tile is 32*V x W*R sites (lane l: V columns, warp w: R rows); the
+// valid region shrinks by one site per level and only the centre OX x OY sites are stored.
+// Level s (1..K) of plane iz-s is computed while plane iz+1 is in flight; each level keeps a
+// 3-plane register queue. The x halo is rounded up to whole vectors so loads and stores stay
+// aligned vectors.
+// ------------------------------------------------------------------------------------------
+template <typename T, bool PER, int K, int V, int R, int W>
+__global__ void __launch_bounds__(32 * W)
+tb3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
+            int ny, int nx, float c0, float c1, int zch, int vec_i) {
+    constexpr int KX = ((K + V - 1) / V) * V;
+    constexpr int EX = 32 * V, OX = EX - 2 * KX;
+    constexpr int EY = W * R, OY = EY - 2 * K;
+    static_assert(OX > 0 && OY > 0, "tile too small for k");
+    __shared__ __align__(16) float edge[2][2][W][EX];  // [buffer][first/last][warp][column]
+    const bool vec = vec_i != 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int gx = blockIdx.x * OX - KX + lane * V;
+    const int gy0 = blockIdx.y * OY - K + w * R;
+    const int z0 = blockIdx.z * zch, z1 = min(z0 + zch, nz);
+    const int64_t P = int64_t(nx) * ny;
+
+    Cols<PER, V> cols;
+    cols.init(gx, nx, vec);
+    int64_t roff[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) roff[r] = int64_t(fix_idx<PER>(gy0 + r, ny)) * nx;
+    uint32_t fixx = 0, fixy = 0;  // Dirichlet: boundary or outside sites keep their value
+    if constexpr (!PER) {
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+            if (gx + j <= 0 || gx + j >= nx - 1) fixx |= 1u << j;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (gy0 + r <= 0 || gy0 + r >= ny - 1) fixy |= 1u << r;
+    }
+    const int lx = lane * V;
+    const bool xwriter = lx >= KX && lx < KX + OX;
+
+    float q[K][3][R][V];
+#pragma unroll
+    for (int s = 0; s < K; ++s)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int j = 0; j < V; ++j) q[s][a][r][j] = 0.f;
+
+    float pre[R][V];
+    auto load_plane = [&](int z, float (&dst)[R][V]) {
+        const T* pl = u + int64_t(fix_idx<PER>(z, nz)) * P;
+#pragma unroll
+        for (int r = 0; r < R; ++r) cols.load(pl + roff[r], vec, dst[r]);
+    };
+    load_plane(z0 - K, pre);
+    int buf = 0;
+
+    for (int iz = z0 - K; iz < z1 + K; ++iz) {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                q[0][0][r][j] = q[0][1][r][j];
+                q[0][1][r][j] = q[0][2][r][j];
+                q[0][2][r][j] = pre[r][j];
+            }
+        if (iz + 1 < z1 + K) load_plane(iz + 1, pre);
+        float res[R][V];
+#pragma unroll
+        for (int s = 1; s <= K; ++s) {
+            const int c = iz - s;
+            float up[V], dn[V];
+            if constexpr (W > 1) {
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    edge[buf][0][w][lx + j] = q[s - 1][1][0][j];
+                    edge[buf][1][w][lx + j] = q[s - 1][1][R - 1][j];
+                }
+                __syncthreads();
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    up[j] = w > 0 ? edge[buf][1][w - 1][lx + j] : q[s - 1][1][0][j];
+                    dn[j] = w < W - 1 ? edge[buf][0][w + 1][lx + j] : q[s - 1][1][R - 1][j];
+                }
+                buf ^= 1;
+            } else {
+#pragma unroll
+                for (int j = 0; j < V; ++j) { up[j] = q[s - 1][1][0][j]; dn[j] = q[s - 1][1][R - 1][j]; }
+            }
+            const bool zfix = !PER && (c <= 0 || c >= nz - 1);
+            const float* bpl = b != nullptr ? b + int64_t(fix_idx<PER>(c, nz)) * P : nullptr;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const float left = __shfl_up_sync(kFull, q[s - 1][1][r][V - 1], 1);
+                const float right = __shfl_down_sync(kFull, q[s - 1][1][r][0], 1);
+                float bv[V];
+                if (bpl != nullptr) cols.load_src(bpl + roff[r], vec, bv);
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    const float ctr = q[s - 1][1][r][j];
+                    const float xm = j > 0 ? q[s - 1][1][r][j - 1] : left;
+                    const float xp = j < V - 1 ? q[s - 1][1][r][j + 1] : right;
+                    const float ym = r > 0 ? q[s - 1][1][r - 1][j] : up[j];
+                    const float yp = r < R - 1 ? q[s - 1][1][r + 1][j] : dn[j];
+                    float v = upd3(c0, c1, ctr, xm, xp, ym, yp, q[s - 1][0][r][j], q[s - 1][2][r][j]);
+                    if (bpl != nullptr) v = __fadd_rn(v, bv[j]);
+                    if constexpr (!PER) {
+                        if (zfix || ((fixy >> r) & 1u) || ((fixx >> j) & 1u)) v = ctr;
+                    }
+                    res[r][j] = v;
+                }
+            }
+            if (s < K) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+#pragma unroll
+                    for (int j = 0; j < V; ++j) {
+                        q[s][0][r][j] = q[s][1][r][j];
+                        q[s][1][r][j] = q[s][2][r][j];
+                        q[s][2][r][j] = res[r][j];
+                    }
+            }
+        }
+        const int c = iz - K;
+        const bool zok = c >= z0 && c < z1 && (PER || (c > 0 && c < nz - 1));
+        if (zok && xwriter) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int row = w * R + r, gy = gy0 + r;
+                if (row >= K && row < K + OY && gy < ny && !((fixy >> r) & 1u))
+                    store_cols<T, V>(o + int64_t(c) * P + int64_t(gy) * nx, gx, nx, vec, fixx,
+                                     res[r]);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// temporal blocking, 2D: warp-synchronous; each warp owns an extended strip of 32*V columns
+// and walks a chunk of rows with a K-level 3-row register queue. No shared memory, no block
+// sync. Strips overlap by 2*KX columns.
+// ------------------------------------------------------------------------------------------
+template <typename T, bool PER, int K, int V, int W>
+__global__ void __launch_bounds__(32 * W)
+tb2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int ny,
+            int nx, float c0, float c1, int ych, int vec_i) {
+    constexpr int KX = ((K + V - 1) / V) * V;
+    constexpr int EX = 32 * V, OX = EX - 2 * KX;
+    static_assert(OX > 0, "strip too narrow for k");
+    const bool vec = vec_i != 0;
+    const int lane = threadIdx.x & 31;
+    const int strip = blockIdx.x * W + (threadIdx.x >> 5);
+    if (strip * OX >= nx) return;  // warp-uniform; no block sync in this kernel
+    const int gx = strip * OX - KX + lane * V;
+    const int y0 = blockIdx.y * ych, y1 = min(y0 + ych, ny);
+
+    Cols<PER, V> cols;
+    cols.init(gx, nx, vec);
+    uint32_t fixx = 0;
+    if constexpr (!PER) {
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+            if (gx + j <= 0 || gx + j >= nx - 1) fixx |= 1u << j;
+    }
+    const int lx = lane * V;
+    const bool xwriter = lx >= KX && lx < KX + OX;
+
+    float q[K][3][V];
+#pragma unroll
+    for (int s = 0; s < K; ++s)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int j = 0; j < V; ++j) q[s][a][j] = 0.f;
+    float pre[V];
+    cols.load(u + int64_t(fix_idx<PER>(y0 - K, ny)) * nx, vec, pre);
+
+    for (int iy = y0 - K; iy < y1 + K; ++iy) {
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+            q[0][0][j] = q[0][1][j];
+            q[0][1][j] = q[0][2][j];
+            q[0][2][j] = pre[j];
+        }
+        if (iy + 1 < y1 + K) cols.load(u + int64_t(fix_idx<PER>(iy + 1, ny)) * nx, vec, pre);
+        float res[V];
+#pragma unroll
+        for (int s = 1; s <= K; ++s) {
+            const int c = iy - s;
+            const bool yfix = !PER && (c <= 0 || c >= ny - 1);
+            const float left = __shfl_up_sync(kFull, q[s - 1][1][V - 1], 1);
+            const float right = __shfl_down_sync(kFull, q[s - 1][1][0], 1);
+            float bv[V];
+            if (b != nullptr) cols.load_src(b + int64_t(fix_idx<PER>(c, ny)) * nx, vec, bv);
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                const float ctr = q[s - 1][1][j];
+                const float xm = j > 0 ? q[s - 1][1][j - 1] : left;
+                const float xp = j < V - 1 ? q[s - 1][1][j + 1] : right;
+                float v = upd2(c0, c1, ctr, xm, xp, q[s - 1][0][j], q[s - 1][2][j]);
+                if (b != nullptr) v = __fadd_rn(v, bv[j]);
+                if constexpr (!PER) {
+                    if (yfix || ((fixx >> j) & 1u)) v = ctr;
+                }
+                res[j] = v;
+            }
+            if (s < K) {
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    q[s][0][j] = q[s][1][j];
+                    q[s][1][j] = q[s][2][j];
+                    q[s][2][j] = res[j];
+                }
+            }
+        }
+        const int c = iy - K;
+        const bool yok = c >= y0 && c < y1 && (PER || (c > 0 && c < ny - 1));
+        if (yok && xwriter) store_cols<T, V>(o + int64_t(c) * nx, gx, nx, vec, fixx, res);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// host launchers
+// ------------------------------------------------------------------------------------------
+static inline int cdiv(long long a, long long b) { return int((a + b - 1) / b); }
+
+static bool aligned_to(const void* p, size_t bytes) {
+    return p == nullptr || (reinterpret_cast<uintptr_t>(p) % bytes) == 0;
+}
+
+int default_chunk(int n_march, long long tiles, int min_len, long long target_ctas) {
+    long long want = (target_ctas + tiles - 1) / std::max(1LL, tiles);
+    want = std::max(1LL, want);
+    int len = cdiv(n_march, want);
+    len = std::max(len, min_len);
+    return std::min(std::max(len, 1), n_march);
+}
+
+template <typename T, bool PER>
+static cudaError_t naive_t(const Launch& L) {
+    const T* u = static_cast<const T*>(L.u);
+    T* o = static_cast<T*>(L.out);
+    if (L.dims == 2) {
+        dim3 blk(32, 8), grd(cdiv(L.nx, 32), cdiv(L.ny, 8));
+        if (grd.y > 65535) return cudaErrorInvalidConfiguration;
+        naive2d_kernel<T, PER><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.ny, L.nx, L.c0, L.c1);
+    } else {
+        dim3 blk(32, 4, 2), grd(cdiv(L.nx, 32), cdiv(L.ny, 4), cdiv(L.nz, 2));
+        if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
+        naive3d_kernel<T, PER><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.nz, L.ny, L.nx, L.c0,
+                                                          L.c1);
+    }
+    return cudaGetLastError();
+}
+
+template <typename T, bool PER, int V>
+static bool vec_ok(const Launch& L) {
+    return L.nx % V == 0 && aligned_to(L.u, sizeof(T) * V) && aligned_to(L.out, sizeof(T) * V) &&
+           aligned_to(L.src, sizeof(float) * V);
+}
+
+template <typename T, bool PER>
+static cudaError_t march_k1_t(const Launch& L) {
+    const T* u = static_cast<const T*>(L.u);
+    T* o = static_cast<T*>(L.out);
+    const long long target = 8LL * sm_count();
+    if (L.dims == 2) {
+        constexpr int V = 16 / sizeof(T), W = 4, RB = 4;
+        const int strips = cdiv(L.nx, 32 * V);
+        const int ych = L.chunk > 0 ? L.chunk
+                                    : default_chunk(L.ny, cdiv(strips, W), 4 * RB, target);
+        dim3 grd(cdiv(strips, W), cdiv(L.ny, ych));
+        if (grd.y > 65535) return cudaErrorInvalidConfiguration;
+        march2d_k1_kernel<T, PER, V, W, RB><<<grd, 32 * W, 0, L.stream>>>(
+            u, o, L.src, L.ny, L.nx, L.c0, L.c1, ych, vec_ok<T, PER, V>(L) ? 1 : 0);
+    } else {
+        constexpr int V = 16 / sizeof(T), R = 2, W = 8;
+        const long long tiles = 1LL * cdiv(L.nx, 32 * V) * cdiv(L.ny, W * R);
+        const int zch = L.chunk > 0 ? L.chunk : default_chunk(L.nz, tiles, 8, target);
+        dim3 grd(cdiv(L.nx, 32 * V), cdiv(L.ny, W * R), cdiv(L.nz, zch));
+        if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
+        march3d_k1_kernel<T, PER, V, R, W><<<grd, 32 * W, 0, L.stream>>>(
+            u, o, L.src, L.nz, L.ny, L.nx, L.c0, L.c1, zch, vec_ok<T, PER, V>(L) ? 1 : 0);
+    }
+    return cudaGetLastError();
+}
+
+template <typename T, bool PER, int K, int V, int R, int W>
+static cudaError_t tb3d_t(const Launch& L) {
+    constexpr int KX = ((K + V - 1) / V) * V, OX = 32 * V - 2 * KX, OY = W * R - 2 * K;
+    const long long tiles = 1LL * cdiv(L.nx, OX) * cdiv(L.ny, OY);
+    const int zch = L.chunk > 0 ? L.chunk
+                                : default_chunk(L.nz, tiles, std::max(8, 4 * K), 4LL * sm_count());
+    dim3 grd(cdiv(L.nx, OX), cdiv(L.ny, OY), cdiv(L.nz, zch));
+    if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
+    tb3d_kernel<T, PER, K, V, R, W><<<grd, 32 * W, 0, L.stream>>>(
+        static_cast<const T*>(L.u), static_cast<T*>(L.out), L.src, L.nz, L.ny, L.nx, L.c0, L.c1,
+        zch, vec_ok<T, PER, V>(L) ? 1 : 0);
+    return cudaGetLastError();
+}
+
+template <typename T, bool PER, int K, int V, int W>
+static cudaError_t tb2d_t(const Launch& L) {
+    constexpr int KX = ((K + V - 1) / V) * V, OX = 32 * V - 2 * KX;
+    const int strips = cdiv(L.nx, OX);
+    const int ych = L.chunk > 0 ? L.chunk
+                                : default_chunk(L.ny, cdiv(strips, W), std::max(16, 8 * K),
+                                                8LL * sm_count());
+    dim3 grd(cdiv(strips, W), cdiv(L.ny, ych));
+    if (grd.y > 65535) return cudaErrorInvalidConfiguration;
+    tb2d_kernel<T, PER, K, V, W><<<grd, 32 * W, 0, L.stream>>>(
+        static_cast<const T*>(L.u), static_cast<T*>(L.out), L.src, L.ny, L.nx, L.c0, L.c1, ych,
+        vec_ok<T, PER, V>(L) ? 1 : 0);
+    return cudaGetLastError();
+}
+
+template <typename T, bool PER>
+static cudaError_t tb_t(const Launch& L) {
+    if (L.dims == 2) {
+        switch (L.k) {
+            case 2: return tb2d_t<T, PER, 2, 4, 4>(L);
+            case 3: return tb2d_t<T, PER, 3, 4, 4>(L);
+            case 4: return tb2d_t<T, PER, 4, 4, 4>(L);
+            case 8: return tb2d_t<T, PER, 8, 4, 4>(L);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (L.k) {
+        case 2: return tb3d_t<T, PER, 2, 4, 2, 16>(L);
+        case 3: return tb3d_t<T, PER, 3, 4, 2, 16>(L);
+        case 4: return tb3d_t<T, PER, 4, 2, 2, 16>(L);
+        case 8: return tb3d_t<T, PER, 8, 2, 1, 32>(L);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+#define PH3_DISPATCH(fn, L)                                                               \
+    do {                                                                                  \
+        switch ((L).storage) {                                                            \
+            case kF32: return (L).periodic ? fn<float, true>(L) : fn<float, false>(L);    \
+            case kF16: return (L).periodic ? fn<__half, true>(L) : fn<__half, false>(L);  \
+            case kBF16:                                                                   \
+                return (L).periodic ? fn<__nv_bfloat16, true>(L)                          \
+                                    : fn<__nv_bfloat16, false>(L);                        \
+            default: return cudaErrorInvalidValue;                                        \
+        }                                                                                 \
+    } while (0)
+
+cudaError_t launch_naive(const Launch& L) { PH3_DISPATCH(naive_t, L); }
+cudaError_t launch_march_k1(const Launch& L) { PH3_DISPATCH(march_k1_t, L); }
+cudaError_t launch_tb(const Launch& L) { PH3_DISPATCH(tb_t, L); }
+
+}  // namespace ph3

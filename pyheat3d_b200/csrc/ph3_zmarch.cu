@@ -1,0 +1,387 @@
+// 3D single-step z-march with TMA plane staging (sm_100a).
+//
+// Functional spec: pyheat3d src/pyheat3d/backends/stencil.cu:101-161 (zmarch3d) — one update of
+// the 7-point stencil per pass, marching along z. This kernel is a new design for B200:
+//
+// * Persistent blocks walk a static list of work items (tile_x, tile_y, z-chunk), ordered with
+//   the chunk slowest so that blocks running at the same time work on neighbouring tiles of the
+//   same planes (halo rows and chunk-edge planes then come from L2, not HBM).
+// * One producer warp streams the planes of each item into a STAGES-deep shared-memory ring with
+//   cp.async.bulk.tensor loads that complete on an mbarrier (transaction bytes): per plane one
+//   TX x TY body box, two TX x 1 halo rows and two HX x TY halo columns, all at wrapped
+//   coordinates for periodic grids (TMA does not wrap; out-of-range Dirichlet halos read zeros
+//   that are never used).
+// * NWC consumer warps keep a register queue along z (below / centre / above), take the
+//   x-neighbours from warp shuffles (lanes 0 and 31 read the halo columns) and the y-neighbours
+//   from registers or the staged plane, and store 16-byte vectors straight to global memory.
+// * Every mbarrier wait is bounded; on expiry the error word is set and the block drains the
+//   loads it issued before returning.
+//
+// Requirements (else the caller uses the plain-load march): nx * sizeof(T) % 16 == 0 and 16-byte
+// aligned buffers.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "ph3_common.cuh"
+#include "ph3_internal.h"
+
+namespace ph3 {
+
+namespace {
+
+constexpr unsigned kFullMask = 0xffffffffu;
+
+template <typename T, int TY, int NWC, int STAGES>
+struct ZmCfg {
+    static constexpr int V = 16 / int(sizeof(T));  // values per lane (one 16-byte vector)
+    static constexpr int TX = 32 * V;              // tile width: 512 bytes per row
+    static constexpr int HX = V;                   // halo column box: 16 bytes
+    static constexpr int RW = TY / NWC;            // rows per consumer warp
+    static_assert(TY % NWC == 0, "rows must split evenly over the consumer warps");
+    static constexpr int BODY_BYTES = (TY + 2) * TX * int(sizeof(T));
+    static constexpr int SIDE_BYTES = TY * HX * int(sizeof(T));
+    static constexpr int STAGE_BYTES = ((BODY_BYTES + 2 * SIDE_BYTES + 127) / 128) * 128;
+    static constexpr int TX_BYTES = BODY_BYTES + 2 * SIDE_BYTES;  // bytes landed per plane
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 16;
+    static constexpr int THREADS = 32 * (NWC + 1);
+};
+
+struct ZmGeom {
+    int nz, ny, nx;
+    int ntx, nty;      // tiles in x and y
+    int zbase, nzi;    // first marched plane and number of marched planes
+    int zch, nchunks;  // chunk length and count
+    int nitems;
+};
+
+template <typename T, bool PER, int TY, int NWC, int STAGES>
+__global__ void __launch_bounds__(32 * (NWC + 1))
+zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
+                  const __grid_constant__ CUtensorMap tm_row,
+                  const __grid_constant__ CUtensorMap tm_side, T* __restrict__ o,
+                  const float* __restrict__ b, ZmGeom g, float c0, float c1, int* err) {
+    using C = ZmCfg<T, TY, NWC, STAGES>;
+    constexpr int V = C::V, TX = C::TX, HX = C::HX, RW = C::RW;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    volatile int* issued = reinterpret_cast<volatile int*>(empty + STAGES);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NWC);
+        }
+        *issued = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    const int64_t P = int64_t(g.nx) * g.ny;
+
+    if (warp == NWC) {
+        // ----------------------------------------------------------------- producer warp
+        if (lane == 0) {
+            prefetch_tmap(&tm_body);
+            prefetch_tmap(&tm_row);
+            prefetch_tmap(&tm_side);
+            uint32_t it = 0;
+            for (int item = blockIdx.x; item < g.nitems; item += gridDim.x) {
+                const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty;
+                const int ch = item / (g.ntx * g.nty);
+                const int x0 = tx * TX, y0 = ty * TY;
+                const int zlo = g.zbase + ch * g.zch;
+                const int zhi = min(zlo + g.zch, g.zbase + g.nzi);
+                int ytop = y0 - 1, ybot = y0 + TY, xl = x0 - HX, xr = x0 + TX;
+                if constexpr (PER) {
+                    ytop = y0 == 0 ? g.ny - 1 : y0 - 1;
+                    ybot = y0 + TY >= g.ny ? 0 : y0 + TY;
+                    xl = x0 == 0 ? g.nx - HX : x0 - HX;
+                    xr = x0 + TX >= g.nx ? 0 : x0 + TX;
+                }
+                for (int p = zlo - 1; p <= zhi; ++p, ++it) {
+                    const int s = it % STAGES;
+                    const uint32_t n = it / STAGES;
+                    if (n > 0 && !mbar_wait(&empty[s], (n & 1u) ^ 1u, err)) return;
+                    int pz = p;
+                    if constexpr (PER) pz = p < 0 ? p + g.nz : (p >= g.nz ? p - g.nz : p);
+                    unsigned char* st = smem + s * C::STAGE_BYTES;
+                    constexpr int ROW = TX * int(sizeof(T));
+                    mbar_arrive_expect_tx(&full[s], C::TX_BYTES);
+                    tma_load_3d(st, &tm_row, x0, ytop, pz, &full[s]);
+                    tma_load_3d(st + ROW, &tm_body, x0, y0, pz, &full[s]);
+                    tma_load_3d(st + (TY + 1) * ROW, &tm_row, x0, ybot, pz, &full[s]);
+                    tma_load_3d(st + C::BODY_BYTES, &tm_side, xl, y0, pz, &full[s]);
+                    tma_load_3d(st + C::BODY_BYTES + C::SIDE_BYTES, &tm_side, xr, y0, pz,
+                                &full[s]);
+                    *issued = int(it + 1);
+                }
+            }
+        }
+        return;
+    }
+
+    // --------------------------------------------------------------------- consumer warps
+    const int r0 = warp * RW;  // first tile row of this warp
+    uint32_t it = 0;
+    bool ok = true;
+    auto body_row = [&](int s, int row) -> const T* {
+        return reinterpret_cast<const T*>(smem + s * C::STAGE_BYTES) + row * TX;
+    };
+    auto side = [&](int s, int right) -> const T* {
+        return reinterpret_cast<const T*>(smem + s * C::STAGE_BYTES + C::BODY_BYTES +
+                                          right * C::SIDE_BYTES);
+    };
+    auto release = [&](int s) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    };
+    auto lds_vec = [&](const T* p, float (&v)[V]) {
+        union { uint4 w; T e[V]; } un;
+        un.w = *reinterpret_cast<const uint4*>(p);
+#pragma unroll
+        for (int j = 0; j < V; ++j) v[j] = to_f(un.e[j]);
+    };
+
+    for (int item = blockIdx.x; item < g.nitems && ok; item += gridDim.x) {
+        const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty;
+        const int ch = item / (g.ntx * g.nty);
+        const int x0 = tx * TX, y0 = ty * TY;
+        const int zlo = g.zbase + ch * g.zch;
+        const int zhi = min(zlo + g.zch, g.zbase + g.nzi);
+        const int gx = x0 + lane * V;
+        // masks of sites this thread must not write
+        uint32_t skipx = 0, skipy = 0;
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+            if (gx + j >= g.nx || (!PER && (gx + j == 0 || gx + j == g.nx - 1))) skipx |= 1u << j;
+#pragma unroll
+        for (int r = 0; r < RW; ++r) {
+            const int gy = y0 + r0 + r;
+            if (gy >= g.ny || (!PER && (gy == 0 || gy == g.ny - 1))) skipy |= 1u << r;
+        }
+        // periodic wrap inside a partial tile: the site after column nx-1 / row ny-1 is the
+        // halo loaded from column 0 / row 0
+        const bool wrapx = PER && (gx + V == g.nx) && lane != 31;
+        float bel[RW][V], ctr[RW][V], abv[RW][V];
+
+        // plane zlo-1: only the own values are needed
+        {
+            const int s = it % STAGES;
+            if (!mbar_wait(&full[s], (it / STAGES) & 1u, err)) { ok = false; break; }
+#pragma unroll
+            for (int r = 0; r < RW; ++r) lds_vec(body_row(s, r0 + r + 1) + lane * V, bel[r]);
+            release(s);
+            ++it;
+        }
+        int sc = it % STAGES;  // stage of the centre plane
+        if (!mbar_wait(&full[sc], (it / STAGES) & 1u, err)) { ok = false; break; }
+#pragma unroll
+        for (int r = 0; r < RW; ++r) lds_vec(body_row(sc, r0 + r + 1) + lane * V, ctr[r]);
+        ++it;
+
+        for (int z = zlo; z < zhi; ++z) {
+            const int sa = it % STAGES;
+            if (!mbar_wait(&full[sa], (it / STAGES) & 1u, err)) { ok = false; break; }
+#pragma unroll
+            for (int r = 0; r < RW; ++r) lds_vec(body_row(sa, r0 + r + 1) + lane * V, abv[r]);
+            // y-neighbours of the first and last rows come from the staged centre plane
+            // periodic partial tile: the row after ny-1 is the halo row loaded from row 0
+            int wrap_r = -1;
+            if (PER && y0 + TY > g.ny) {
+                const int rr = g.ny - 1 - (y0 + r0);
+                if (rr >= 0 && rr < RW) wrap_r = rr;
+            }
+            float up[V], dn[V], wdn[V];
+            lds_vec(body_row(sc, r0) + lane * V, up);
+            lds_vec(body_row(sc, wrap_r == RW - 1 ? TY + 1 : r0 + RW + 1) + lane * V, dn);
+            if (wrap_r >= 0 && wrap_r < RW - 1) lds_vec(body_row(sc, TY + 1) + lane * V, wdn);
+            const T* sl = side(sc, 0);
+            const T* sr = side(sc, 1);
+#pragma unroll
+            for (int r = 0; r < RW; ++r) {
+                const int gy = y0 + r0 + r;
+                const float left = __shfl_up_sync(kFullMask, ctr[r][V - 1], 1);
+                const float right = __shfl_down_sync(kFullMask, ctr[r][0], 1);
+                float hl = 0.f, hr = 0.f;
+                if (lane == 0) hl = to_f(sl[(r0 + r) * HX + HX - 1]);
+                if (lane == 31 || wrapx) hr = to_f(sr[(r0 + r) * HX]);
+                float bv[V];
+                if (b != nullptr) {
+                    const float* bp = b + int64_t(z) * P + int64_t(min(gy, g.ny - 1)) * g.nx +
+                                      min(gx, g.nx - V);
+#pragma unroll
+                    for (int q = 0; q < V / 4; ++q) {
+                        const float4 t = __ldg(reinterpret_cast<const float4*>(bp) + q);
+                        bv[4 * q] = t.x; bv[4 * q + 1] = t.y; bv[4 * q + 2] = t.z; bv[4 * q + 3] = t.w;
+                    }
+                }
+                float out[V];
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    const float xm = j > 0 ? ctr[r][j - 1] : (lane == 0 ? hl : left);
+                    const float xp = j < V - 1 ? ctr[r][j + 1]
+                                               : ((lane == 31 || wrapx) ? hr : right);
+                    const float ym = r > 0 ? ctr[r - 1][j] : up[j];
+                    float yp = dn[j];
+                    if (r < RW - 1) yp = r == wrap_r ? wdn[j] : ctr[r + 1][j];
+                    float v = upd3(c0, c1, ctr[r][j], xm, xp, ym, yp, bel[r][j], abv[r][j]);
+                    if (b != nullptr) v = __fadd_rn(v, bv[j]);
+                    out[j] = v;
+                }
+                if (!((skipy >> r) & 1u)) {
+                    T* dst = o + int64_t(z) * P + int64_t(gy) * g.nx + gx;
+                    if (skipx == 0) {
+                        st_vec<T, V>(dst, out);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < V; ++j)
+                            if (!((skipx >> j) & 1u)) dst[j] = from_f<T>(out[j]);
+                    }
+                }
+            }
+            release(sc);
+#pragma unroll
+            for (int r = 0; r < RW; ++r)
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    bel[r][j] = ctr[r][j];
+                    ctr[r][j] = abv[r][j];
+                }
+            sc = sa;
+            ++it;
+        }
+        if (!ok) break;
+        release(sc);  // plane zhi
+    }
+
+    if (!ok) {
+        // a wait expired: drain the loads this block issued so no copy lands after exit
+        if (warp == 0 && lane == 0) {
+            const int n_issued = *issued;
+            for (int k = int(it); k < n_issued; ++k) {
+                const int s = k % STAGES;
+                if (!mbar_wait(&full[s], (uint32_t(k) / STAGES) & 1u, err)) break;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+template <typename T>
+CUtensorMapDataType tm_dtype() {
+    if constexpr (sizeof(T) == 4) return CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    else if constexpr (std::is_same_v<T, __half>) return CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    else return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+}
+
+template <typename T>
+bool make_map(CUtensorMap* m, const void* base, int nz, int ny, int nx, int bx, int by) {
+    auto enc = get_encode();
+    if (enc == nullptr) return false;
+    cuuint64_t dims[3] = {cuuint64_t(nx), cuuint64_t(ny), cuuint64_t(nz)};
+    cuuint64_t strides[2] = {cuuint64_t(nx) * sizeof(T), cuuint64_t(nx) * ny * sizeof(T)};
+    cuuint32_t box[3] = {cuuint32_t(bx), cuuint32_t(by), 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    return enc(m, tm_dtype<T>(), 3, const_cast<void*>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T, bool PER, int TY, int NWC, int STAGES>
+cudaError_t zmarch_t(const Launch& L) {
+    using C = ZmCfg<T, TY, NWC, STAGES>;
+    auto kern = zmarch_tma_kernel<T, PER, TY, NWC, STAGES>;
+    static int blocks_per_sm[64] = {0};  // per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (blocks_per_sm[dev] == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             C::SMEM);
+        if (e != cudaSuccess) return e;
+        int nb = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, C::THREADS, C::SMEM);
+        if (e != cudaSuccess) return e;
+        blocks_per_sm[dev] = std::max(1, nb);
+    }
+    CUtensorMap tb, tr, ts;
+    if (!make_map<T>(&tb, L.u, L.nz, L.ny, L.nx, C::TX, TY) ||
+        !make_map<T>(&tr, L.u, L.nz, L.ny, L.nx, C::TX, 1) ||
+        !make_map<T>(&ts, L.u, L.nz, L.ny, L.nx, C::HX, TY))
+        return cudaErrorInvalidValue;
+    ZmGeom g;
+    g.nz = L.nz; g.ny = L.ny; g.nx = L.nx;
+    g.ntx = (L.nx + C::TX - 1) / C::TX;
+    g.nty = (L.ny + TY - 1) / TY;
+    g.zbase = L.periodic ? 0 : 1;
+    g.nzi = L.periodic ? L.nz : L.nz - 2;
+    if (g.nzi <= 0) return cudaSuccess;
+    const long long tiles = 1LL * g.ntx * g.nty;
+    // chunk: bounded so that one chunk of the field (read + write) stays well inside L2
+    int zch = L.chunk;
+    if (zch <= 0) {
+        const long long plane_bytes = 1LL * L.nx * L.ny * sizeof(T);
+        const long long cap = std::max(8LL, (32LL << 20) / std::max(1LL, 2 * plane_bytes));
+        zch = int(std::min<long long>(cap, 64));
+        zch = std::min(zch, default_chunk(g.nzi, tiles, 8, 4LL * sm_count() * blocks_per_sm[dev]));
+        zch = std::max(1, std::min(zch, g.nzi));
+    }
+    g.zch = zch;
+    g.nchunks = (g.nzi + zch - 1) / zch;
+    const long long nitems = tiles * g.nchunks;
+    if (nitems > (1LL << 30)) return cudaErrorInvalidValue;
+    g.nitems = int(nitems);
+    const int grid = int(std::min<long long>(nitems, 1LL * sm_count() * blocks_per_sm[dev]));
+    kern<<<grid, C::THREADS, C::SMEM, L.stream>>>(tb, tr, ts, static_cast<T*>(L.out), L.src, g,
+                                                  L.c0, L.c1, L.err);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool zmarch_tma_supported(const Launch& L) {
+    const size_t es = L.storage == kF32 ? 4 : 2;
+    auto al = [](const void* p) { return p == nullptr || reinterpret_cast<uintptr_t>(p) % 16 == 0; };
+    return L.dims == 3 && (size_t(L.nx) * es) % 16 == 0 && al(L.u) && al(L.out) && al(L.src) &&
+           L.nx >= int(16 / es) && get_encode() != nullptr;
+}
+
+cudaError_t launch_zmarch_tma(const Launch& L) {
+    constexpr int TY = 16, NWC = 8, ST = 6;
+    switch (L.storage) {
+        case kF32:
+            return L.periodic ? zmarch_t<float, true, TY, NWC, ST>(L)
+                              : zmarch_t<float, false, TY, NWC, ST>(L);
+        case kF16:
+            return L.periodic ? zmarch_t<__half, true, TY, NWC, ST>(L)
+                              : zmarch_t<__half, false, TY, NWC, ST>(L);
+        case kBF16:
+            return L.periodic ? zmarch_t<__nv_bfloat16, true, TY, NWC, ST>(L)
+                              : zmarch_t<__nv_bfloat16, false, TY, NWC, ST>(L);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace ph3

@@ -1,0 +1,133 @@
+"""``B200Stepper``: the pyheat3d ``Stepper`` of this backend.
+
+Same contract as pyheat3d's CuPy stepper (``src/pyheat3d/backends/cupy_backend.py:115-213``):
+two device buffers hold the ping-pong pair, ``step(n)`` runs ``n // k`` fused passes and
+``n % k`` single steps and is asynchronous, ``get()`` returns a host float32 array. Differences:
+the buffers are torch CUDA tensors, the kernels are called through the ``libph3b200`` C ABI on
+torch's current stream, and a Jacobi source term is supported (``source=``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .contract import Stepper
+
+_TORCH_DTYPE_NAMES = {"float32": "float32", "float16": "float16", "bfloat16": "bfloat16"}
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+class B200Stepper(Stepper):
+    """sm_100a stencil stepper. Subclasses fix ``kind`` ("naive", "march", "tb"), K, storage."""
+
+    kind = "march"
+    K = 1
+    storage = "float32"
+
+    def __init__(self, u0: np.ndarray, stencil, source: np.ndarray | None = None):
+        super().__init__(u0, stencil, source)
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device")
+        self._lib = _lib.lib()  # fails loudly when the extension is missing
+        if self.kind == "march" and self.dims not in (2, 3):  # pragma: no cover
+            raise ValueError("march needs a 2D or 3D grid")
+        self.steps_per_pass = self.K if self.kind == "tb" else 1
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        dt = getattr(torch, _TORCH_DTYPE_NAMES[self.storage])
+        host = torch.from_numpy(np.ascontiguousarray(u0, dtype=np.float32))
+        # float32 -> storage on the device: round to nearest even, as cupy_backend.py:103-107
+        self.a = host.to(self.device).to(dt).contiguous()
+        self.b = self.a.clone()
+        self.src = None
+        if source is not None:
+            if tuple(source.shape) != self.shape:
+                raise ValueError(f"source shape {source.shape} != field shape {self.shape}")
+            self.src = torch.from_numpy(
+                np.ascontiguousarray(source, dtype=np.float32)).to(self.device)
+        self._c0 = float(np.float32(self.c0))
+        self._c1 = float(np.float32(self.c1))
+        sh = self.shape
+        self._nz, self._ny, self._nx = (1, sh[0], sh[1]) if self.dims == 2 else sh
+        self._variant = _lib.VARIANT[self.kind]
+        self._k = self.K if self.kind == "tb" else 1
+        self.tile = {"kind": self.kind, "k": self._k}
+        self._in_b = ctypes.c_int(0)
+
+    # -- stepping ------------------------------------------------------------------------
+    def step(self, n: int = 1) -> None:
+        if n < 0:
+            raise ValueError("n must be >= 0")
+        torch = _torch()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        src = self.src.data_ptr() if self.src is not None else None
+        _lib.check(self._lib.ph3_advance(
+            self.dims, self._nz, self._ny, self._nx, _lib.STORAGE[self.storage],
+            _lib.BC[self.bc], self._c0, self._c1, self._variant, self._k,
+            self.a.data_ptr(), self.b.data_ptr(), src, int(n), stream,
+            ctypes.byref(self._in_b)))
+        if self._in_b.value:
+            self.a, self.b = self.b, self.a
+        self.steps_done += n
+
+    def get(self, out=None) -> np.ndarray:
+        """Current state as a host float32 array.
+
+        ``out`` (optional): a host float32 torch tensor of the field's shape, typically pinned;
+        the device-to-host copy then lands there (asynchronously for pinned memory, followed by
+        a stream synchronisation) and its NumPy view is returned.
+        """
+        if out is None:
+            return self.a.float().cpu().numpy()
+        torch = _torch()
+        src = self.a if self.a.dtype == torch.float32 else self.a.float()
+        out.copy_(src, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return out.numpy()
+
+    def set_state(self, u) -> None:
+        """Replace the state by ``u`` (NumPy array or host / device torch tensor of the shape).
+
+        Host tensors in pinned memory are copied asynchronously on the current stream. With
+        Dirichlet boundaries both ping-pong buffers receive the new boundary values.
+        """
+        torch = _torch()
+        t = torch.from_numpy(np.ascontiguousarray(u, dtype=np.float32)) if isinstance(
+            u, np.ndarray) else u
+        if tuple(t.shape) != self.shape:
+            raise ValueError(f"state shape {tuple(t.shape)} != field shape {self.shape}")
+        if self.a.dtype == t.dtype:
+            self.a.copy_(t, non_blocking=True)
+        else:
+            self.a.copy_(t.to(self.device, non_blocking=True).to(self.a.dtype))
+        if not self.periodic:
+            self.b.copy_(self.a)
+
+    def get_tensor(self):
+        """Current state as the device tensor (storage dtype); no copy."""
+        return self.a
+
+    def synchronize(self) -> None:
+        _torch().cuda.synchronize(self.device)
+
+    def close(self) -> None:
+        self.a = self.b = self.src = None
+
+
+def make(kind: str, storage: str = "float32", K: int = 1) -> type[B200Stepper]:
+    """A ``B200Stepper`` subclass for a kernel family, storage type and K (cupy_backend.py:207)."""
+    if kind not in _lib.VARIANT:
+        raise ValueError(f"unknown kind {kind!r}")
+    if storage not in _lib.STORAGE:
+        raise ValueError(f"unknown storage {storage!r}")
+    _lib.lib()  # availability probe: raises if the extension cannot be loaded
+    return type(f"B200_{kind}{K}_{storage}", (B200Stepper,),
+                {"kind": kind, "storage": storage, "K": K})
