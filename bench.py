@@ -60,6 +60,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--no-variants", action="store_true", help="skip the per-variant table")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--n", type=int, default=N3,
+                    help="grid edge of the headline field (512; smaller only for profiling)")
     return ap.parse_args()
 
 
@@ -285,7 +287,7 @@ def run_b200(a: argparse.Namespace) -> None:
     hbm_peak, peak_kind = peaks()
     copy_bw = copy_bandwidth(torch)
     stencil = heat_stencil(3, R3, "periodic")
-    u0 = field(N3, 3, seed=rank)
+    u0 = field(a.n, 3, seed=rank)
     cells = u0.size
 
     # ---- value: K solves, field resident in HBM
@@ -371,9 +373,9 @@ def run_b200(a: argparse.Namespace) -> None:
             "value": round(value, 2), "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": round(secs / K * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "3D 512^3 fp32 periodic heat, r=0.95/6, uniform[0,1) seed 0 "
-                                   "(rank r: seed r), b200/zmarch",
-                       "grid": [N3, N3, N3], "bc": "periodic", "storage": "float32",
+            "config": {"workload": f"3D {a.n}^3 fp32 periodic heat, r=0.95/6, uniform[0,1) "
+                                   "seed 0 (rank r: seed r), b200/zmarch",
+                       "grid": [a.n, a.n, a.n], "bc": "periodic", "storage": "float32",
                        "time_steps_per_step": T, "units": "site updates (all cells)",
                        "l2": "inputs larger than L2 (512 MiB field vs 126 MB L2)",
                        "parallelism": f"replicas x{ws}"},

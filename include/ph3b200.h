@@ -49,6 +49,12 @@ extern "C" {
 #define PH3_VARIANT_MARCH 1 /* single-step march: TMA z-march in 3D, y-march in 2D */
 #define PH3_VARIANT_TB 2    /* temporal blocking, k fused steps per pass */
 
+/* kernel families of the tuning table */
+#define PH3_KERNEL_ZMARCH 0 /* 3D TMA z-march, k = 1 */
+#define PH3_KERNEL_MARCH 1  /* plain-load single-step march (2D y-march, 3D unaligned) */
+#define PH3_KERNEL_TB 2     /* temporal blocking, k in {2, 3, 4, 8} */
+#define PH3_KERNEL_NAIVE 3  /* one site per thread (no configurations) */
+
 /* Library version (major*10000 + minor*100 + patch). */
 int ph3_version(void);
 
@@ -109,6 +115,22 @@ int ph3_tb2d(const void* u, void* out, const float* src, int ny, int nx, int k, 
 int ph3_advance(int dims, int nz, int ny, int nx, int storage, int bc, float c0, float c1,
                 int variant, int k, void* a, void* b, const float* src, int64_t nsteps,
                 void* stream, int* in_b);
+
+/*
+ * Tuning table (no counterpart in the reference, whose tile constants are module globals that
+ * bench/tune.py monkey-patches, cupy_backend.py:50-70). Every family has a few compiled tile
+ * configurations; the table holds, per (kernel, dims, storage, k), the configuration index and
+ * the march chunk (planes per work item in 3D, rows per block in 2D) that the launches use.
+ * -1 / 0 mean "built-in default". The table is process-wide and applies to all devices.
+ *
+ * ph3_tune_count: number of configurations of (kernel, dims, k); 0 if none.
+ * ph3_tune_name:  name of configuration `cfg` ("" and an error if out of range).
+ * ph3_tune_set / ph3_tune_get: write / read one table entry.
+ */
+int ph3_tune_count(int kernel, int dims, int k);
+const char* ph3_tune_name(int kernel, int dims, int k, int cfg);
+int ph3_tune_set(int kernel, int dims, int storage, int k, int cfg, int chunk);
+int ph3_tune_get(int kernel, int dims, int storage, int k, int* cfg, int* chunk);
 
 #ifdef __cplusplus
 }

@@ -31,7 +31,14 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "ph3_tb2d": (_i, [_p, _p, _p, _i, _i, _i, _f, _f, _i, _i, _i, _p]),
     "ph3_advance": (_i, [_i, _i, _i, _i, _i, _i, _f, _f, _i, _i, _p, _p, _p, _i64, _p,
                          ctypes.POINTER(_i)]),
+    "ph3_tune_count": (_i, [_i, _i, _i]),
+    "ph3_tune_name": (ctypes.c_char_p, [_i, _i, _i, _i]),
+    "ph3_tune_set": (_i, [_i, _i, _i, _i, _i, _i]),
+    "ph3_tune_get": (_i, [_i, _i, _i, _i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
 }
+
+#: tuning-table kernel families (include/ph3b200.h PH3_KERNEL_*)
+KERNEL = {"zmarch": 0, "march": 1, "tb": 2, "naive": 3}
 
 _lock = threading.Lock()
 _lib: ctypes.CDLL | None = None

@@ -2,6 +2,7 @@
 // Declarations and conventions: include/ph3b200.h.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <mutex>
@@ -68,13 +69,48 @@ int check_ptrs(const void* u, const void* out, const float* src) {
     return PH3_OK;
 }
 
+// ------------------------------------------------------------------------ tuning table
+constexpr int kMaxK = 8;
+std::atomic<int> g_tune_cfg[kNumFamilies][2][3][kMaxK + 1];
+std::atomic<int> g_tune_chunk[kNumFamilies][2][3][kMaxK + 1];
+std::once_flag g_tune_once;
+
+void tune_init() {
+    std::call_once(g_tune_once, [] {
+        for (int f = 0; f < kNumFamilies; ++f)
+            for (int d = 0; d < 2; ++d)
+                for (int s = 0; s < 3; ++s)
+                    for (int k = 0; k <= kMaxK; ++k) {
+                        g_tune_cfg[f][d][s][k].store(-1);
+                        g_tune_chunk[f][d][s][k].store(0);
+                    }
+    });
+}
+
+int family_count(int family, int dims, int k, const char** names, int max) {
+    switch (family) {
+        case kFamZmarch: return dims == 3 && k == 1 ? zmarch_configs(names, max) : 0;
+        case kFamMarch: return k == 1 ? march_configs(dims, names, max) : 0;
+        case kFamTb: return tb_configs(dims, k, names, max);
+        default: return 0;
+    }
+}
+
+// Fill cfg / chunk of a launch from the table (an explicit chunk argument wins).
+void apply_tune(Launch& L, int family) {
+    tune_init();
+    const int d = L.dims - 2, s = L.storage, k = L.k < 0 || L.k > kMaxK ? 0 : L.k;
+    L.cfg = g_tune_cfg[family][d][s][k].load(std::memory_order_relaxed);
+    if (L.chunk <= 0) L.chunk = g_tune_chunk[family][d][s][k].load(std::memory_order_relaxed);
+}
+
 Launch make(int dims, int nz, int ny, int nx, int storage, int bc, float c0, float c1,
             const void* u, void* out, const float* src, int k, int chunk, void* stream) {
     Launch L;
     L.u = u; L.out = out; L.src = src;
     L.dims = dims; L.nz = dims == 2 ? 1 : nz; L.ny = ny; L.nx = nx;
     L.periodic = bc == PH3_PERIODIC; L.storage = storage;
-    L.c0 = c0; L.c1 = c1; L.k = k; L.chunk = chunk;
+    L.c0 = c0; L.c1 = c1; L.k = k; L.chunk = chunk; L.cfg = -1;
     L.stream = static_cast<cudaStream_t>(stream);
     L.err = status_ptr();
     return L;
@@ -86,10 +122,19 @@ int finish(cudaError_t e, const char* what) {
     return PH3_OK;
 }
 
-cudaError_t launch_single(const Launch& L, int variant) {
+cudaError_t launch_single(Launch L, int variant) {
     if (variant == PH3_VARIANT_NAIVE) return launch_naive(L);
-    if (L.dims == 3 && zmarch_tma_supported(L)) return launch_zmarch_tma(L);
+    if (L.dims == 3 && zmarch_tma_supported(L)) {
+        apply_tune(L, kFamZmarch);
+        return launch_zmarch_tma(L);
+    }
+    apply_tune(L, kFamMarch);
     return launch_march_k1(L);
+}
+
+cudaError_t launch_tb_tuned(Launch L) {
+    apply_tune(L, kFamTb);
+    return launch_tb(L);
 }
 
 }  // namespace
@@ -175,7 +220,8 @@ int ph3_ymarch2d(const void* u, void* out, const float* src, int ny, int nx, flo
     if (rc == PH3_OK) rc = check_ptrs(u, out, src);
     if (rc != PH3_OK) return rc;
     return finish(
-        launch_march_k1(make(2, 1, ny, nx, storage, bc, c0, c1, u, out, src, 1, chunk, stream)),
+        launch_single(make(2, 1, ny, nx, storage, bc, c0, c1, u, out, src, 1, chunk, stream),
+                      PH3_VARIANT_MARCH),
         "ymarch2d launch");
 }
 
@@ -187,7 +233,7 @@ static int tb_common(int dims, const void* u, void* out, const float* src, int n
     if (k != 2 && k != 3 && k != 4 && k != 8)
         return fail(PH3_EINVAL, "tb k must be one of 2, 3, 4, 8, got %d", k);
     return finish(
-        launch_tb(make(dims, nz, ny, nx, storage, bc, c0, c1, u, out, src, k, chunk, stream)),
+        launch_tb_tuned(make(dims, nz, ny, nx, storage, bc, c0, c1, u, out, src, k, chunk, stream)),
         dims == 3 ? "tb3d launch" : "tb2d launch");
 }
 
@@ -226,7 +272,7 @@ int ph3_advance(int dims, int nz, int ny, int nx, int storage, int bc, float c0,
     const int64_t rest = k > 1 ? nsteps % k : nsteps;
     for (int64_t i = 0; i < passes; ++i) {
         L.u = cur; L.out = nxt;
-        cudaError_t e = launch_tb(L);
+        cudaError_t e = launch_tb_tuned(L);
         if (e != cudaSuccess) return cuda_fail(e, "tb launch");
         void* t = const_cast<void*>(cur); cur = nxt; nxt = t; swaps ^= 1;
     }
@@ -239,6 +285,58 @@ int ph3_advance(int dims, int nz, int ny, int nx, int storage, int bc, float c0,
     }
     *in_b = swaps;
     g_err[0] = '\0';
+    return PH3_OK;
+}
+
+static thread_local char g_name[64];
+
+static int check_tune_key(int kernel, int dims, int storage, int k) {
+    if (kernel < 0 || kernel >= kNumFamilies) return fail(PH3_EINVAL, "unknown kernel %d", kernel);
+    if (dims != 2 && dims != 3) return fail(PH3_EINVAL, "dims must be 2 or 3, got %d", dims);
+    if (storage < PH3_FLOAT32 || storage > PH3_BFLOAT16)
+        return fail(PH3_EINVAL, "storage must be 0, 1 or 2, got %d", storage);
+    if (k < 1 || k > kMaxK) return fail(PH3_EINVAL, "k must be in 1..%d, got %d", kMaxK, k);
+    return PH3_OK;
+}
+
+int ph3_tune_count(int kernel, int dims, int k) {
+    if (check_tune_key(kernel, dims, PH3_FLOAT32, k) != PH3_OK) return 0;
+    return family_count(kernel, dims, k, nullptr, 0);
+}
+
+const char* ph3_tune_name(int kernel, int dims, int k, int cfg) {
+    g_name[0] = '\0';
+    if (check_tune_key(kernel, dims, PH3_FLOAT32, k) != PH3_OK) return g_name;
+    const char* names[16] = {nullptr};
+    const int n = family_count(kernel, dims, k, names, 16);
+    if (cfg < 0 || cfg >= n || cfg >= 16 || names[cfg] == nullptr) {
+        fail(PH3_EINVAL, "configuration %d out of range (%d)", cfg, n);
+        return g_name;
+    }
+    snprintf(g_name, sizeof(g_name), "%s", names[cfg]);
+    return g_name;
+}
+
+int ph3_tune_set(int kernel, int dims, int storage, int k, int cfg, int chunk) {
+    int rc = check_tune_key(kernel, dims, storage, k);
+    if (rc != PH3_OK) return rc;
+    const int n = family_count(kernel, dims, k, nullptr, 0);
+    if (cfg >= n) return fail(PH3_EINVAL, "configuration %d out of range (%d)", cfg, n);
+    if (chunk < 0) return fail(PH3_EINVAL, "chunk must be >= 0");
+    tune_init();
+    g_tune_cfg[kernel][dims - 2][storage][k].store(cfg < 0 ? -1 : cfg);
+    g_tune_chunk[kernel][dims - 2][storage][k].store(chunk);
+    g_err[0] = '\0';
+    return PH3_OK;
+}
+
+int ph3_tune_get(int kernel, int dims, int storage, int k, int* cfg, int* chunk) {
+    int rc = check_tune_key(kernel, dims, storage, k);
+    if (rc != PH3_OK) return rc;
+    if (cfg == nullptr || chunk == nullptr) return fail(PH3_EINVAL, "cfg and chunk must be non-null");
+    tune_init();
+    *cfg = g_tune_cfg[kernel][dims - 2][storage][k].load();
+    *chunk = g_tune_chunk[kernel][dims - 2][storage][k].load();
     return PH3_OK;
 }
 

@@ -56,6 +56,17 @@ __device__ __forceinline__ void ld_vec(const T* __restrict__ p, float (&v)[V]) {
     }
 }
 
+// V storage values from shared (or any generic) memory as one 4/8/16-byte access.
+template <typename T, int V>
+__device__ __forceinline__ void ld_vec_shared(const T* p, float (&v)[V]) {
+    constexpr int B = int(sizeof(T)) * V;
+    using W = typename VecBytes<B>::type;
+    union { W w; T e[V]; } u;
+    u.w = *reinterpret_cast<const W*>(p);
+#pragma unroll
+    for (int j = 0; j < V; ++j) v[j] = to_f(u.e[j]);
+}
+
 template <typename T, int V>
 __device__ __forceinline__ void st_vec(T* __restrict__ p, const float (&v)[V]) {
     constexpr int B = int(sizeof(T)) * V;
@@ -70,6 +81,52 @@ __device__ __forceinline__ void st_vec(T* __restrict__ p, const float (&v)[V]) {
     }
 }
 
+// 16 bytes of storage <-> float2 pairs (8 B: 2 fp32; 4 x 16-bit pairs), round to nearest even.
+template <typename T> struct Pack16;
+template <> struct Pack16<float> {
+    static constexpr int NP = 2;
+    __device__ __forceinline__ static void unpack(const uint4& w, float2 (&v)[NP]) {
+        v[0] = make_float2(__uint_as_float(w.x), __uint_as_float(w.y));
+        v[1] = make_float2(__uint_as_float(w.z), __uint_as_float(w.w));
+    }
+    __device__ __forceinline__ static uint4 pack(const float2 (&v)[NP]) {
+        return make_uint4(__float_as_uint(v[0].x), __float_as_uint(v[0].y),
+                          __float_as_uint(v[1].x), __float_as_uint(v[1].y));
+    }
+};
+template <> struct Pack16<__nv_bfloat16> {
+    static constexpr int NP = 4;
+    __device__ __forceinline__ static float2 cvt(uint32_t w) {
+        return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+    }
+    __device__ __forceinline__ static uint32_t rnd(float2 v) {
+        __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+    __device__ __forceinline__ static void unpack(const uint4& w, float2 (&v)[NP]) {
+        v[0] = cvt(w.x); v[1] = cvt(w.y); v[2] = cvt(w.z); v[3] = cvt(w.w);
+    }
+    __device__ __forceinline__ static uint4 pack(const float2 (&v)[NP]) {
+        return make_uint4(rnd(v[0]), rnd(v[1]), rnd(v[2]), rnd(v[3]));
+    }
+};
+template <> struct Pack16<__half> {
+    static constexpr int NP = 4;
+    __device__ __forceinline__ static float2 cvt(uint32_t w) {
+        return __half22float2(*reinterpret_cast<const __half2*>(&w));
+    }
+    __device__ __forceinline__ static uint32_t rnd(float2 v) {
+        __half2 h = __floats2half2_rn(v.x, v.y);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+    __device__ __forceinline__ static void unpack(const uint4& w, float2 (&v)[NP]) {
+        v[0] = cvt(w.x); v[1] = cvt(w.y); v[2] = cvt(w.z); v[3] = cvt(w.w);
+    }
+    __device__ __forceinline__ static uint4 pack(const float2 (&v)[NP]) {
+        return make_uint4(rnd(v[0]), rnd(v[1]), rnd(v[2]), rnd(v[3]));
+    }
+};
+
 // ------------------------------------------------------------------------------------------
 // canonical-order stencil arithmetic
 // ------------------------------------------------------------------------------------------
@@ -83,6 +140,37 @@ __device__ __forceinline__ float upd3(float c0, float c1, float ctr, float xm, f
                                       float ym, float yp, float zm, float zp) {
     const float s = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym, yp)), __fadd_rn(zm, zp));
     return __fadd_rn(__fmul_rn(c0, ctr), __fmul_rn(c1, s));
+}
+
+// Packed fp32x2 add / multiply (sm_100a `add.rn.f32x2`, `mul.rn.f32x2`): each lane rounds
+// exactly like __fadd_rn / __fmul_rn, so a packed chain is bit-identical to the scalar one.
+union F2 {
+    float2 f;
+    unsigned long long u;
+};
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    F2 x, y, r;
+    x.f = a; y.f = b;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.u) : "l"(x.u), "l"(y.u));
+    return r.f;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    F2 x, y, r;
+    x.f = a; y.f = b;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.u) : "l"(x.u), "l"(y.u));
+    return r.f;
+}
+
+// Two neighbouring sites of one row: the same canonical-order update as upd3 / upd2, packed.
+__device__ __forceinline__ float2 upd3_x2(float2 c0, float2 c1, float2 ctr, float2 xm, float2 xp,
+                                          float2 ym, float2 yp, float2 zm, float2 zp) {
+    const float2 s = add2(add2(add2(xm, xp), add2(ym, yp)), add2(zm, zp));
+    return add2(mul2(c0, ctr), mul2(c1, s));
+}
+__device__ __forceinline__ float2 upd2_x2(float2 c0, float2 c1, float2 ctr, float2 xm, float2 xp,
+                                          float2 ym, float2 yp) {
+    const float2 s = add2(add2(xm, xp), add2(ym, yp));
+    return add2(mul2(c0, ctr), mul2(c1, s));
 }
 
 __device__ __forceinline__ int wrap_idx(int i, int n) {
@@ -181,6 +269,22 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, 
         " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
+}
+
+// Untiled bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16),
+// completion counted on an mbarrier (bytes).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes),
+        "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Barrier over the first `threads` threads of the block (named barrier `id`, 1..15).
+__device__ __forceinline__ void named_sync(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 
 __device__ __forceinline__ void prefetch_tmap(const void* tmap) {

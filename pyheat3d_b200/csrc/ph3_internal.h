@@ -20,6 +20,7 @@ struct Launch {
     float c0, c1;
     int k;              // fused time steps (1 for single-step kernels)
     int chunk;          // march chunk length (planes in 3D, rows in 2D); <= 0 picks a default
+    int cfg;            // compiled tile configuration of the family; < 0 picks the default
     cudaStream_t stream;
     int* err;           // device status word for bounded waits (may be null)
 };
@@ -30,6 +31,18 @@ cudaError_t launch_march_k1(const Launch& L);   // register march, k = 1, any sh
 cudaError_t launch_tb(const Launch& L);         // temporal blocking, k in {2,3,4,8}
 cudaError_t launch_zmarch_tma(const Launch& L); // 3D TMA z-march, k = 1, aligned shapes
 bool zmarch_tma_supported(const Launch& L);
+cudaError_t launch_tbbulk(const Launch& L);     // 3D tb with a bulk-copy ring, aligned shapes
+bool tbbulk_supported(const Launch& L);
+int tbbulk_configs(int k, const char** names, int max);
+
+// Kernel families with selectable compiled configurations (the tuning table's first index).
+enum Family : int { kFamZmarch = 0, kFamMarch = 1, kFamTb = 2, kFamNaive = 3, kNumFamilies = 4 };
+
+// Names of the compiled configurations of a family for (dims, k); returns how many there are.
+// names may be null. Implemented by the translation unit that owns the family.
+int zmarch_configs(const char** names, int max);
+int march_configs(int dims, const char** names, int max);
+int tb_configs(int dims, int k, const char** names, int max);
 
 // Number of streaming multiprocessors of the current device (cached per device).
 int sm_count();

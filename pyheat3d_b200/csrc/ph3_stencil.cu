@@ -630,7 +630,7 @@ static cudaError_t march_k1_t(const Launch& L) {
     T* o = static_cast<T*>(L.out);
     const long long target = 8LL * sm_count();
     if (L.dims == 2) {
-        constexpr int V = 16 / sizeof(T), W = 4, RB = 4;
+        constexpr int V = 16 / sizeof(T), W = 4, RB = sizeof(T) == 4 ? 4 : 2;
         const int strips = cdiv(L.nx, 32 * V);
         const int ych = L.chunk > 0 ? L.chunk
                                     : default_chunk(L.ny, cdiv(strips, W), 4 * RB, target);
@@ -713,6 +713,24 @@ static cudaError_t tb_t(const Launch& L) {
 
 cudaError_t launch_naive(const Launch& L) { PH3_DISPATCH(naive_t, L); }
 cudaError_t launch_march_k1(const Launch& L) { PH3_DISPATCH(march_k1_t, L); }
-cudaError_t launch_tb(const Launch& L) { PH3_DISPATCH(tb_t, L); }
+
+static cudaError_t launch_tb_plain(const Launch& L) { PH3_DISPATCH(tb_t, L); }
+
+cudaError_t launch_tb(const Launch& L) {
+    if (L.dims == 3 && tbbulk_supported(L)) return launch_tbbulk(L);
+    return launch_tb_plain(L);
+}
+
+int march_configs(int dims, const char** names, int max) {
+    if (names != nullptr && max > 0) names[0] = dims == 2 ? "V16B_W4_RB4" : "V16B_R2_W8";
+    return 1;
+}
+
+int tb_configs(int dims, int k, const char** names, int max) {
+    if (dims == 3) return tbbulk_configs(k, names, max);
+    if (k != 2 && k != 3 && k != 4 && k != 8) return 0;
+    if (names != nullptr && max > 0) names[0] = "V4_W4";
+    return 1;
+}
 
 }  // namespace ph3

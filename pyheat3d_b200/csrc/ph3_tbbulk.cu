@@ -1,0 +1,422 @@
+// 3D temporal blocking with a bulk-copy plane ring (sm_100a).
+//
+// Functional spec: pyheat3d src/pyheat3d/backends/stencil.cu:178-281 (tb3d) — k updates per
+// DRAM pass by a (z, t) wavefront over overlapped xy tiles; intermediate levels stay in fp32 and
+// are rounded to storage once per pass (src/pyheat3d/validation.py:168-183 emulates this).
+//
+// Design for B200:
+// * Persistent blocks walk a static list of work items (tile_x, tile_y, z-chunk), chunk
+//   slowest. The chunk length is chosen on the host to balance the items over the resident
+//   blocks against the 2k warm-up planes every chunk costs.
+// * The level-0 planes of the block's extended tile (EX x EY sites, EX = 32 lanes x V) stream
+//   into a STAGES-deep shared-memory ring with cp.async.bulk row copies (issued by the lanes of
+//   warp 0, one row each) that complete on an mbarrier. A row is one copy, split in two where
+//   it crosses the periodic seam (untiled bulk copies take any 16-byte aligned source address,
+//   so the wrap costs nothing); the ring holds the wrapped extended tile exactly. A stage is
+//   refilled one iteration after it was read: the named barriers of that iteration already
+//   order every read before the refill, so no "empty" barrier is needed.
+// * The warps own R rows x V columns each. Per level they keep two planes in registers
+//   (c-1 and c; c+1 is the plane the previous level produced in the same iteration), take the
+//   x-neighbours from warp shuffles, the y-neighbours from their own rows and, at the warp's
+//   first/last row, from a shared-memory edge exchange behind a named barrier. Math is packed
+//   fp32x2, bit-identical to the scalar chain.
+// * Waits are bounded. If one expires the block records the error, stops waiting (but keeps
+//   every barrier so no warp is left behind), skips its stores and drains its copies.
+//
+// Requirements (else the plain-load tb3d kernel runs): nx * sizeof(T) % 16 == 0, 16-byte aligned
+// buffers, nx >= 16 / sizeof(T).
+#include <algorithm>
+
+#include "ph3_common.cuh"
+#include "ph3_internal.h"
+
+namespace ph3 {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct TbGeom {
+    int nz, ny, nx;
+    int ntx, nty;
+    int zch, nch;
+    int nitems;
+};
+
+template <typename T, int K, int V, int R, int NWC, int STAGES>
+struct TbCfg {
+    static constexpr int G = 16 / int(sizeof(T));        // 16-byte granule in elements
+    static constexpr int KX = ((K + G - 1) / G) * G;     // x halo, whole granules
+    static constexpr int EX = 32 * V, OX = EX - 2 * KX;  // extended / stored tile width
+    static constexpr int EY = NWC * R, OY = EY - 2 * K;  // extended / stored tile height
+    static_assert(OX > 0 && OY > 0 && EX % G == 0, "tile too small for k");
+    static constexpr int ROW_BYTES = EX * int(sizeof(T));
+    static constexpr int PLANE_BYTES = EY * ROW_BYTES;
+    static constexpr int EDGE_FLOATS = 2 * 2 * NWC * EX;  // [buffer][first/last][warp][column]
+    static constexpr int SMEM = STAGES * PLANE_BYTES + EDGE_FLOATS * 4 + STAGES * 8;
+    static constexpr int THREADS = 32 * NWC;
+};
+
+// V storage values of one lane from shared memory, as V/2 float2 pairs.
+template <typename T, int V>
+__device__ __forceinline__ void lds_lane(const T* p, float2 (&v)[V / 2]) {
+    float f[V];
+    ld_vec_shared<T, V>(p, f);
+#pragma unroll
+    for (int q = 0; q < V / 2; ++q) v[q] = make_float2(f[2 * q], f[2 * q + 1]);
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void stg_lane(T* p, const float2 (&v)[V / 2]) {
+    float f[V];
+#pragma unroll
+    for (int q = 0; q < V / 2; ++q) { f[2 * q] = v[q].x; f[2 * q + 1] = v[q].y; }
+    st_vec<T, V>(p, f);
+}
+
+template <typename T, bool PER, int K, int V, int R, int NWC, int STAGES>
+__global__ void __launch_bounds__(32 * NWC, 1)
+tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b,
+                 TbGeom g, float c0, float c1, int* err) {
+    using C = TbCfg<T, K, V, R, NWC, STAGES>;
+    constexpr int NP = V / 2, EX = C::EX, EY = C::EY, KX = C::KX, OX = C::OX, OY = C::OY;
+    static_assert(V % 2 == 0, "lanes hold whole float2 pairs");
+    static_assert(STAGES >= 2, "ring needs two stages");
+    extern __shared__ __align__(128) unsigned char smem[];
+    T* ring = reinterpret_cast<T*>(smem);
+    float* edge = reinterpret_cast<float*>(smem + STAGES * C::PLANE_BYTES);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * C::PLANE_BYTES +
+                                                 C::EDGE_FLOATS * 4);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const int64_t P = int64_t(g.nx) * g.ny;
+
+    // ------------------------------------------------------------------ plane issue (warp 0)
+    // Warp 0 keeps an issue cursor over the same (item, plane) sequence the block consumes and
+    // refills each stage one plane after it was consumed: by then every warp has passed the
+    // named barrier of that iteration, so all reads of the stage are done.
+    int is_item = blockIdx.x, is_iz = 0, is_zend = 0;
+    uint32_t is_it = 0;
+    auto cursor_item = [&](int item) {
+        if (item >= g.nitems) return;
+        const int ch = item / (g.ntx * g.nty);
+        const int z0 = ch * g.zch, z1 = min(z0 + g.zch, g.nz);
+        is_iz = z0 - K;
+        is_zend = z1 + K;
+    };
+    auto issue_next = [&]() {
+        if (is_item >= g.nitems) return;
+        const int tx = is_item % g.ntx, ty = (is_item / g.ntx) % g.nty;
+        const int xs = tx * OX - KX, ys = ty * OY - K;
+        const int s = is_it % STAGES;
+        const int pz = PER ? wrap_idx(is_iz, g.nz) : clamp_idx(is_iz, 0, g.nz - 1);
+        if (lane == 0) mbar_arrive_expect_tx(&full[s], C::PLANE_BYTES);
+        __syncwarp();
+        T* plane = ring + s * (EY * EX);
+        for (int r = lane; r < EY; r += 32) {
+            const int gy = PER ? wrap_idx(ys + r, g.ny) : clamp_idx(ys + r, 0, g.ny - 1);
+            const T* row = u + int64_t(pz) * P + int64_t(gy) * g.nx;
+            T* dst = plane + r * EX;
+            int done = 0;
+            while (done < EX) {
+                const int x = xs + done;
+                int src, len;
+                if (PER) {
+                    src = wrap_idx(x, g.nx);
+                    len = min(EX - done, g.nx - src);
+                } else if (x < 0) {  // outside the domain: any in-range data will do
+                    src = 0;
+                    len = min(min(EX - done, -x), g.nx);
+                } else if (x >= g.nx) {
+                    src = 0;
+                    len = min(EX - done, g.nx);
+                } else {
+                    src = x;
+                    len = min(EX - done, g.nx - x);
+                }
+                bulk_load(dst + done, row + src, uint32_t(len) * sizeof(T), &full[s]);
+                done += len;
+            }
+        }
+        ++is_it;
+        if (++is_iz >= is_zend) {
+            is_item += gridDim.x;
+            cursor_item(is_item);
+        }
+    };
+    if (warp == 0) {
+        cursor_item(is_item);
+        for (int i = 0; i < STAGES - 1; ++i) issue_next();
+    }
+
+    // ------------------------------------------------------------------------ all warps
+    const float2 c0v = make_float2(c0, c0), c1v = make_float2(c1, c1);
+    const int lx = lane * V;
+    uint32_t it = 0, waited = 0;  // planes consumed / planes whose copies were seen to land
+    int buf = 0;
+    bool ok = true;
+    float2 A[K][R][NP], B[K][R][NP];  // level s: plane c (A) and c-1 (B)
+
+    for (int item = blockIdx.x; item < g.nitems; item += gridDim.x) {
+        const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty, ch = item / (g.ntx * g.nty);
+        const int xs = tx * OX - KX, ys = ty * OY - K;
+        const int z0 = ch * g.zch, z1 = min(z0 + g.zch, g.nz);
+        const int gx = xs + lx, gy0 = ys + warp * R;
+        uint32_t fixx = 0, fixy = 0;  // Dirichlet: boundary / outside sites keep their value
+        if constexpr (!PER) {
+#pragma unroll
+            for (int j = 0; j < V; ++j)
+                if (gx + j <= 0 || gx + j >= g.nx - 1) fixx |= 1u << j;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (gy0 + r <= 0 || gy0 + r >= g.ny - 1) fixy |= 1u << r;
+        }
+        const bool xwriter = lx >= KX && lx < KX + OX && gx < g.nx;
+        const int bcol = PER ? wrap_idx(gx, g.nx) : clamp_idx(gx, 0, g.nx - V);
+#pragma unroll
+        for (int s = 0; s < K; ++s)
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int p = 0; p < NP; ++p) A[s][r][p] = B[s][r][p] = make_float2(0.f, 0.f);
+
+        for (int iz = z0 - K; iz < z1 + K; ++iz, ++it) {
+            if (warp == 0 && ok) issue_next();
+            const int s = it % STAGES;
+            if (ok) {
+                if (mbar_wait(&full[s], (it / STAGES) & 1u, err)) ++waited;
+                else ok = false;
+            }
+            float2 N[R][NP];
+            const T* plane = ring + s * (EY * EX);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (ok) {
+                    lds_lane<T, V>(plane + (warp * R + r) * EX + lx, N[r]);
+                } else {
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) N[r][p] = make_float2(0.f, 0.f);
+                }
+            }
+
+#pragma unroll
+            for (int lev = 1; lev <= K; ++lev) {
+                const int c = iz - lev;
+                // y-neighbours of the first / last row: exchange with the adjacent warps
+                float* eb = edge + buf * (2 * NWC * EX);
+                {
+                    float* w0 = eb + warp * EX + lx;
+                    float* w1 = eb + (NWC + warp) * EX + lx;
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) {
+                        *reinterpret_cast<float2*>(w0 + 2 * p) = A[lev - 1][0][p];
+                        *reinterpret_cast<float2*>(w1 + 2 * p) = A[lev - 1][R - 1][p];
+                    }
+                }
+                named_sync(1, NWC * 32);
+                float2 up[NP], dn[NP];
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    up[p] = warp > 0 ? *reinterpret_cast<const float2*>(
+                                           eb + (NWC + warp - 1) * EX + lx + 2 * p)
+                                     : A[lev - 1][0][p];
+                    dn[p] = warp < NWC - 1
+                                ? *reinterpret_cast<const float2*>(eb + (warp + 1) * EX + lx + 2 * p)
+                                : A[lev - 1][R - 1][p];
+                }
+                buf ^= 1;
+                const bool zfix = !PER && (c <= 0 || c >= g.nz - 1);
+                const float* bpl = nullptr;
+                if (b != nullptr)
+                    bpl = b + int64_t(PER ? wrap_idx(c, g.nz) : clamp_idx(c, 0, g.nz - 1)) * P;
+                float2 res[R][NP];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const float left = __shfl_up_sync(kFull, A[lev - 1][r][NP - 1].y, 1);
+                    const float right = __shfl_down_sync(kFull, A[lev - 1][r][0].x, 1);
+                    float2 bv[NP];
+                    if (bpl != nullptr) {
+                        const int gy = PER ? wrap_idx(gy0 + r, g.ny) : clamp_idx(gy0 + r, 0, g.ny - 1);
+                        float f[V];
+                        ld_vec<float, V>(bpl + int64_t(gy) * g.nx + bcol, f);
+#pragma unroll
+                        for (int p = 0; p < NP; ++p) bv[p] = make_float2(f[2 * p], f[2 * p + 1]);
+                    }
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) {
+                        const float2 ctr = A[lev - 1][r][p];
+                        const float2 xm = make_float2(p > 0 ? A[lev - 1][r][p - 1].y : left, ctr.x);
+                        const float2 xp = make_float2(ctr.y, p < NP - 1 ? A[lev - 1][r][p + 1].x : right);
+                        const float2 ym = r > 0 ? A[lev - 1][r - 1][p] : up[p];
+                        const float2 yp = r < R - 1 ? A[lev - 1][r + 1][p] : dn[p];
+                        float2 v = upd3_x2(c0v, c1v, ctr, xm, xp, ym, yp, B[lev - 1][r][p], N[r][p]);
+                        if (bpl != nullptr) v = add2(v, bv[p]);
+                        if constexpr (!PER) {
+                            const bool fr = zfix || ((fixy >> r) & 1u);
+                            if (fr || ((fixx >> (2 * p)) & 1u)) v.x = ctr.x;
+                            if (fr || ((fixx >> (2 * p + 1)) & 1u)) v.y = ctr.y;
+                        }
+                        res[r][p] = v;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) {
+                        B[lev - 1][r][p] = A[lev - 1][r][p];
+                        A[lev - 1][r][p] = N[r][p];
+                        N[r][p] = res[r][p];
+                    }
+            }
+            // N now holds level K of plane iz - K
+            const int c = iz - K;
+            if (ok && xwriter && c >= z0 && c < z1 && (PER || (c > 0 && c < g.nz - 1))) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int row = warp * R + r, gy = gy0 + r;
+                    if (row < K || row >= K + OY || gy >= g.ny || ((fixy >> r) & 1u)) continue;
+                    T* dst = o + int64_t(c) * P + int64_t(gy) * g.nx + gx;
+                    if (fixx == 0 && gx + V <= g.nx) {
+                        stg_lane<T, V>(dst, N[r]);
+                    } else {
+#pragma unroll
+                        for (int p = 0; p < NP; ++p) {
+                            const int j = 2 * p;
+                            if (gx + j < g.nx && !((fixx >> j) & 1u)) dst[j] = from_f<T>(N[r][p].x);
+                            if (gx + j + 1 < g.nx && !((fixx >> (j + 1)) & 1u))
+                                dst[j + 1] = from_f<T>(N[r][p].y);
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    // every plane warp 0 issued must land before the block exits (normally all were consumed)
+    if (warp == 0 && lane == 0) {
+        for (uint32_t k = waited; k < is_it; ++k)
+            if (!mbar_wait(&full[k % STAGES], (k / STAGES) & 1u, err)) break;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------------
+
+// Chunk length minimising the per-block critical path ceil(items / blocks) * (zch + 2k).
+int balanced_chunk(int nz, long long tiles, long long blocks, int k) {
+    int best = nz;
+    double best_cost = 1e300;
+    const int max_ch = std::max(1, nz / std::max(2 * k, 4));
+    for (int nch = 1; nch <= max_ch; ++nch) {
+        const int zch = (nz + nch - 1) / nch;
+        const int real_nch = (nz + zch - 1) / zch;
+        const long long items = tiles * real_nch;
+        const double waves = double((items + blocks - 1) / blocks);
+        const double cost = waves * (zch + 2.0 * k);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = zch;
+        }
+    }
+    return best;
+}
+
+template <typename T, bool PER, int K, int V, int R, int NWC, int STAGES>
+cudaError_t tbbulk_t(const Launch& L) {
+    using C = TbCfg<T, K, V, R, NWC, STAGES>;
+    auto kern = tb3d_bulk_kernel<T, PER, K, V, R, NWC, STAGES>;
+    static int blocks_per_sm[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (blocks_per_sm[dev] == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             C::SMEM);
+        if (e != cudaSuccess) return e;
+        int nb = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, C::THREADS, C::SMEM);
+        if (e != cudaSuccess) return e;
+        if (nb < 1) return cudaErrorInvalidConfiguration;
+        blocks_per_sm[dev] = nb;
+    }
+    TbGeom g;
+    g.nz = L.nz; g.ny = L.ny; g.nx = L.nx;
+    g.ntx = (L.nx + C::OX - 1) / C::OX;
+    g.nty = (L.ny + C::OY - 1) / C::OY;
+    const long long tiles = 1LL * g.ntx * g.nty;
+    const long long blocks = 1LL * sm_count() * blocks_per_sm[dev];
+    g.zch = L.chunk > 0 ? std::min(L.chunk, L.nz) : balanced_chunk(L.nz, tiles, blocks, K);
+    g.nch = (L.nz + g.zch - 1) / g.zch;
+    const long long items = tiles * g.nch;
+    if (items > (1LL << 30)) return cudaErrorInvalidValue;
+    g.nitems = int(items);
+    const int grid = int(std::min(items, blocks));
+    kern<<<grid, C::THREADS, C::SMEM, L.stream>>>(static_cast<const T*>(L.u),
+                                                  static_cast<T*>(L.out), L.src, g, L.c0, L.c1,
+                                                  L.err);
+    return cudaGetLastError();
+}
+
+// Compiled configurations per k: (V values per lane, R rows per warp, consumer warps, stages).
+struct TbEntry {
+    int k;
+    const char* name;
+};
+const TbEntry kTbNames[] = {
+    {2, "V4_R2_W16_S4"}, {2, "V4_R4_W8_S4"},  {3, "V4_R2_W16_S4"}, {3, "V4_R4_W8_S4"},
+    {4, "V4_R2_W16_S4"}, {4, "V2_R2_W16_S6"}, {8, "V2_R2_W16_S6"}, {8, "V2_R4_W8_S6"},
+};
+
+template <typename T, bool PER>
+cudaError_t tbbulk_dispatch(const Launch& L) {
+    const int cfg = L.cfg < 0 ? 0 : L.cfg;
+    switch (L.k) {
+        case 2:
+            return cfg == 1 ? tbbulk_t<T, PER, 2, 4, 4, 8, 4>(L) : tbbulk_t<T, PER, 2, 4, 2, 16, 4>(L);
+        case 3:
+            return cfg == 1 ? tbbulk_t<T, PER, 3, 4, 4, 8, 4>(L) : tbbulk_t<T, PER, 3, 4, 2, 16, 4>(L);
+        case 4:
+            return cfg == 1 ? tbbulk_t<T, PER, 4, 2, 2, 16, 6>(L) : tbbulk_t<T, PER, 4, 4, 2, 16, 4>(L);
+        case 8:
+            return cfg == 1 ? tbbulk_t<T, PER, 8, 2, 4, 8, 6>(L) : tbbulk_t<T, PER, 8, 2, 2, 16, 6>(L);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+int tbbulk_configs(int k, const char** names, int max) {
+    int n = 0;
+    for (const auto& e : kTbNames)
+        if (e.k == k) {
+            if (names != nullptr && n < max) names[n] = e.name;
+            ++n;
+        }
+    return n;
+}
+
+bool tbbulk_supported(const Launch& L) {
+    const size_t es = L.storage == kF32 ? 4 : 2;
+    auto al = [](const void* p) { return p == nullptr || reinterpret_cast<uintptr_t>(p) % 16 == 0; };
+    return L.dims == 3 && (size_t(L.nx) * es) % 16 == 0 && L.nx >= int(16 / es) && al(L.u) &&
+           al(L.out) && al(L.src);
+}
+
+cudaError_t launch_tbbulk(const Launch& L) {
+    switch (L.storage) {
+        case kF32: return L.periodic ? tbbulk_dispatch<float, true>(L) : tbbulk_dispatch<float, false>(L);
+        case kF16: return L.periodic ? tbbulk_dispatch<__half, true>(L) : tbbulk_dispatch<__half, false>(L);
+        case kBF16:
+            return L.periodic ? tbbulk_dispatch<__nv_bfloat16, true>(L)
+                              : tbbulk_dispatch<__nv_bfloat16, false>(L);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace ph3

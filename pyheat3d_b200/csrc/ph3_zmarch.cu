@@ -57,14 +57,24 @@ struct ZmGeom {
     int nitems;
 };
 
+// Blocks per SM the register budget is sized for (the ring's shared memory allows as many).
+template <typename T, int TY, int NWC>
+constexpr int zm_min_blocks() {
+    constexpr int RW = TY / NWC;
+    if (NWC >= 16) return sizeof(T) == 4 ? 2 : 1;
+    if (sizeof(T) == 4) return RW >= 4 ? 2 : 3;
+    return RW >= 2 ? 1 : 3;
+}
+
 template <typename T, bool PER, int TY, int NWC, int STAGES>
-__global__ void __launch_bounds__(32 * (NWC + 1))
+__global__ void __launch_bounds__(32 * (NWC + 1), zm_min_blocks<T, TY, NWC>())
 zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                   const __grid_constant__ CUtensorMap tm_row,
                   const __grid_constant__ CUtensorMap tm_side, T* __restrict__ o,
                   const float* __restrict__ b, ZmGeom g, float c0, float c1, int* err) {
     using C = ZmCfg<T, TY, NWC, STAGES>;
     constexpr int V = C::V, TX = C::TX, HX = C::HX, RW = C::RW;
+    static_assert(V % 2 == 0, "lanes hold whole float2 pairs");
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE_BYTES);
     uint64_t* empty = full + STAGES;
@@ -126,11 +136,15 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
     }
 
     // --------------------------------------------------------------------- consumer warps
-    const int r0 = warp * RW;  // first tile row of this warp
+    using PK = Pack16<T>;
+    constexpr int NP = PK::NP;  // float2 pairs per lane (V / 2)
+    const int r0 = warp * RW;   // first tile row of this warp
+    const float2 c0v = make_float2(c0, c0), c1v = make_float2(c1, c1);
     uint32_t it = 0;
     bool ok = true;
-    auto body_row = [&](int s, int row) -> const T* {
-        return reinterpret_cast<const T*>(smem + s * C::STAGE_BYTES) + row * TX;
+    auto stage_row = [&](int s, int row) -> const uint4* {
+        return reinterpret_cast<const uint4*>(smem + s * C::STAGE_BYTES + row * TX * int(sizeof(T))) +
+               lane;
     };
     auto side = [&](int s, int right) -> const T* {
         return reinterpret_cast<const T*>(smem + s * C::STAGE_BYTES + C::BODY_BYTES +
@@ -139,12 +153,6 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
     auto release = [&](int s) {
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
-    };
-    auto lds_vec = [&](const T* p, float (&v)[V]) {
-        union { uint4 w; T e[V]; } un;
-        un.w = *reinterpret_cast<const uint4*>(p);
-#pragma unroll
-        for (int j = 0; j < V; ++j) v[j] = to_f(un.e[j]);
     };
 
     for (int item = blockIdx.x; item < g.nitems && ok; item += gridDim.x) {
@@ -167,80 +175,80 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
         // periodic wrap inside a partial tile: the site after column nx-1 / row ny-1 is the
         // halo loaded from column 0 / row 0
         const bool wrapx = PER && (gx + V == g.nx) && lane != 31;
-        float bel[RW][V], ctr[RW][V], abv[RW][V];
+        int wrap_r = -1;
+        if (PER && y0 + TY > g.ny) {
+            const int rr = g.ny - 1 - (y0 + r0);
+            if (rr >= 0 && rr < RW) wrap_r = rr;
+        }
+        float2 bel[RW][NP], ctr[RW][NP], abv[RW][NP];
 
         // plane zlo-1: only the own values are needed
         {
             const int s = it % STAGES;
             if (!mbar_wait(&full[s], (it / STAGES) & 1u, err)) { ok = false; break; }
 #pragma unroll
-            for (int r = 0; r < RW; ++r) lds_vec(body_row(s, r0 + r + 1) + lane * V, bel[r]);
+            for (int r = 0; r < RW; ++r) PK::unpack(*stage_row(s, r0 + r + 1), bel[r]);
             release(s);
             ++it;
         }
         int sc = it % STAGES;  // stage of the centre plane
         if (!mbar_wait(&full[sc], (it / STAGES) & 1u, err)) { ok = false; break; }
 #pragma unroll
-        for (int r = 0; r < RW; ++r) lds_vec(body_row(sc, r0 + r + 1) + lane * V, ctr[r]);
+        for (int r = 0; r < RW; ++r) PK::unpack(*stage_row(sc, r0 + r + 1), ctr[r]);
         ++it;
 
         for (int z = zlo; z < zhi; ++z) {
             const int sa = it % STAGES;
             if (!mbar_wait(&full[sa], (it / STAGES) & 1u, err)) { ok = false; break; }
 #pragma unroll
-            for (int r = 0; r < RW; ++r) lds_vec(body_row(sa, r0 + r + 1) + lane * V, abv[r]);
-            // y-neighbours of the first and last rows come from the staged centre plane
-            // periodic partial tile: the row after ny-1 is the halo row loaded from row 0
-            int wrap_r = -1;
-            if (PER && y0 + TY > g.ny) {
-                const int rr = g.ny - 1 - (y0 + r0);
-                if (rr >= 0 && rr < RW) wrap_r = rr;
-            }
-            float up[V], dn[V], wdn[V];
-            lds_vec(body_row(sc, r0) + lane * V, up);
-            lds_vec(body_row(sc, wrap_r == RW - 1 ? TY + 1 : r0 + RW + 1) + lane * V, dn);
-            if (wrap_r >= 0 && wrap_r < RW - 1) lds_vec(body_row(sc, TY + 1) + lane * V, wdn);
+            for (int r = 0; r < RW; ++r) PK::unpack(*stage_row(sa, r0 + r + 1), abv[r]);
+            // y-neighbours of the warp's first and last rows come from the staged centre plane
+            float2 up[NP], dn[NP], wdn[NP];
+            PK::unpack(*stage_row(sc, r0), up);
+            PK::unpack(*stage_row(sc, wrap_r == RW - 1 ? TY + 1 : r0 + RW + 1), dn);
+            if (wrap_r >= 0 && wrap_r < RW - 1) PK::unpack(*stage_row(sc, TY + 1), wdn);
             const T* sl = side(sc, 0);
             const T* sr = side(sc, 1);
 #pragma unroll
             for (int r = 0; r < RW; ++r) {
                 const int gy = y0 + r0 + r;
-                const float left = __shfl_up_sync(kFullMask, ctr[r][V - 1], 1);
-                const float right = __shfl_down_sync(kFullMask, ctr[r][0], 1);
-                float hl = 0.f, hr = 0.f;
-                if (lane == 0) hl = to_f(sl[(r0 + r) * HX + HX - 1]);
-                if (lane == 31 || wrapx) hr = to_f(sr[(r0 + r) * HX]);
-                float bv[V];
+                const float left = __shfl_up_sync(kFullMask, ctr[r][NP - 1].y, 1);
+                const float right = __shfl_down_sync(kFullMask, ctr[r][0].x, 1);
+                const float xlv = lane == 0 ? to_f(sl[(r0 + r) * HX + HX - 1]) : left;
+                const float xrv = (lane == 31 || wrapx) ? to_f(sr[(r0 + r) * HX]) : right;
+                float2 bv[NP];
                 if (b != nullptr) {
-                    const float* bp = b + int64_t(z) * P + int64_t(min(gy, g.ny - 1)) * g.nx +
-                                      min(gx, g.nx - V);
+                    const float4* bp = reinterpret_cast<const float4*>(
+                        b + int64_t(z) * P + int64_t(min(gy, g.ny - 1)) * g.nx + min(gx, g.nx - V));
 #pragma unroll
-                    for (int q = 0; q < V / 4; ++q) {
-                        const float4 t = __ldg(reinterpret_cast<const float4*>(bp) + q);
-                        bv[4 * q] = t.x; bv[4 * q + 1] = t.y; bv[4 * q + 2] = t.z; bv[4 * q + 3] = t.w;
+                    for (int q = 0; q < NP / 2; ++q) {
+                        const float4 t4 = __ldg(bp + q);
+                        bv[2 * q] = make_float2(t4.x, t4.y);
+                        bv[2 * q + 1] = make_float2(t4.z, t4.w);
                     }
                 }
-                float out[V];
+                float2 out[NP];
 #pragma unroll
-                for (int j = 0; j < V; ++j) {
-                    const float xm = j > 0 ? ctr[r][j - 1] : (lane == 0 ? hl : left);
-                    const float xp = j < V - 1 ? ctr[r][j + 1]
-                                               : ((lane == 31 || wrapx) ? hr : right);
-                    const float ym = r > 0 ? ctr[r - 1][j] : up[j];
-                    float yp = dn[j];
-                    if (r < RW - 1) yp = r == wrap_r ? wdn[j] : ctr[r + 1][j];
-                    float v = upd3(c0, c1, ctr[r][j], xm, xp, ym, yp, bel[r][j], abv[r][j]);
-                    if (b != nullptr) v = __fadd_rn(v, bv[j]);
-                    out[j] = v;
+                for (int p = 0; p < NP; ++p) {
+                    const float2 xm = make_float2(p > 0 ? ctr[r][p - 1].y : xlv, ctr[r][p].x);
+                    const float2 xp = make_float2(ctr[r][p].y, p < NP - 1 ? ctr[r][p + 1].x : xrv);
+                    const float2 ym = r > 0 ? ctr[r - 1][p] : up[p];
+                    float2 yp = dn[p];
+                    if (r < RW - 1) yp = r == wrap_r ? wdn[p] : ctr[r + 1][p];
+                    float2 v = upd3_x2(c0v, c1v, ctr[r][p], xm, xp, ym, yp, bel[r][p], abv[r][p]);
+                    if (b != nullptr) v = add2(v, bv[p]);
+                    out[p] = v;
                 }
                 if (!((skipy >> r) & 1u)) {
                     T* dst = o + int64_t(z) * P + int64_t(gy) * g.nx + gx;
                     if (skipx == 0) {
-                        st_vec<T, V>(dst, out);
+                        *reinterpret_cast<uint4*>(dst) = PK::pack(out);
                     } else {
 #pragma unroll
-                        for (int j = 0; j < V; ++j)
-                            if (!((skipx >> j) & 1u)) dst[j] = from_f<T>(out[j]);
+                        for (int p = 0; p < NP; ++p) {
+                            if (!((skipx >> (2 * p)) & 1u)) dst[2 * p] = from_f<T>(out[p].x);
+                            if (!((skipx >> (2 * p + 1)) & 1u)) dst[2 * p + 1] = from_f<T>(out[p].y);
+                        }
                     }
                 }
             }
@@ -248,9 +256,9 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
 #pragma unroll
             for (int r = 0; r < RW; ++r)
 #pragma unroll
-                for (int j = 0; j < V; ++j) {
-                    bel[r][j] = ctr[r][j];
-                    ctr[r][j] = abv[r][j];
+                for (int p = 0; p < NP; ++p) {
+                    bel[r][p] = ctr[r][p];
+                    ctr[r][p] = abv[r][p];
                 }
             sc = sa;
             ++it;
@@ -368,18 +376,38 @@ bool zmarch_tma_supported(const Launch& L) {
            L.nx >= int(16 / es) && get_encode() != nullptr;
 }
 
+// Compiled z-march configurations: rows per tile (TY), consumer warps (NWC), ring stages.
+static const char* kZmNames[] = {"TY16_W8_S6", "TY8_W8_S8", "TY32_W8_S4", "TY16_W16_S6",
+                                 "TY8_W4_S8"};
+constexpr int kZmCount = 5;
+
+int zmarch_configs(const char** names, int max) {
+    for (int i = 0; i < kZmCount && names != nullptr && i < max; ++i) names[i] = kZmNames[i];
+    return kZmCount;
+}
+
+template <typename T, bool PER>
+static cudaError_t zmarch_cfg(const Launch& L) {
+    // defaults: fp32 -> 16 rows x 8 warps; 16-bit -> 8 rows x 8 warps (one row per warp keeps
+    // the 8-value lanes at low register count)
+    int cfg = L.cfg;
+    if (cfg < 0 || cfg >= kZmCount) cfg = sizeof(T) == 4 ? 0 : 1;
+    switch (cfg) {
+        case 0: return zmarch_t<T, PER, 16, 8, 6>(L);
+        case 1: return zmarch_t<T, PER, 8, 8, 8>(L);
+        case 2: return zmarch_t<T, PER, 32, 8, 4>(L);
+        case 3: return zmarch_t<T, PER, 16, 16, 6>(L);
+        default: return zmarch_t<T, PER, 8, 4, 8>(L);
+    }
+}
+
 cudaError_t launch_zmarch_tma(const Launch& L) {
-    constexpr int TY = 16, NWC = 8, ST = 6;
     switch (L.storage) {
-        case kF32:
-            return L.periodic ? zmarch_t<float, true, TY, NWC, ST>(L)
-                              : zmarch_t<float, false, TY, NWC, ST>(L);
-        case kF16:
-            return L.periodic ? zmarch_t<__half, true, TY, NWC, ST>(L)
-                              : zmarch_t<__half, false, TY, NWC, ST>(L);
+        case kF32: return L.periodic ? zmarch_cfg<float, true>(L) : zmarch_cfg<float, false>(L);
+        case kF16: return L.periodic ? zmarch_cfg<__half, true>(L) : zmarch_cfg<__half, false>(L);
         case kBF16:
-            return L.periodic ? zmarch_t<__nv_bfloat16, true, TY, NWC, ST>(L)
-                              : zmarch_t<__nv_bfloat16, false, TY, NWC, ST>(L);
+            return L.periodic ? zmarch_cfg<__nv_bfloat16, true>(L)
+                              : zmarch_cfg<__nv_bfloat16, false>(L);
         default: return cudaErrorInvalidValue;
     }
 }

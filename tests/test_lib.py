@@ -94,3 +94,25 @@ def test_product_path_does_not_import_the_oracle():
     for py in pkg.rglob("*.py"):
         text = py.read_text()
         assert not re.search(r"^\s*(from|import)\s+oracle\b", text, flags=re.M), py
+
+
+def test_tuning_table_roundtrip(lib):
+    K = _lib.KERNEL
+    assert lib.ph3_tune_count(K["zmarch"], 3, 1) >= 2
+    assert lib.ph3_tune_count(K["zmarch"], 2, 1) == 0
+    for k in (2, 3, 4, 8):
+        n = lib.ph3_tune_count(K["tb"], 3, k)
+        assert n >= 1
+        names = {lib.ph3_tune_name(K["tb"], 3, k, c).decode() for c in range(n)}
+        assert len(names) == n and all(names)
+    assert lib.ph3_tune_name(K["tb"], 3, 2, 99) == b""
+    cfg, chunk = ctypes.c_int(7), ctypes.c_int(7)
+    _lib.check(lib.ph3_tune_get(K["tb"], 3, 0, 4, ctypes.byref(cfg), ctypes.byref(chunk)))
+    assert (cfg.value, chunk.value) == (-1, 0)
+    _lib.check(lib.ph3_tune_set(K["tb"], 3, 0, 4, 1, 48))
+    _lib.check(lib.ph3_tune_get(K["tb"], 3, 0, 4, ctypes.byref(cfg), ctypes.byref(chunk)))
+    assert (cfg.value, chunk.value) == (1, 48)
+    _lib.check(lib.ph3_tune_set(K["tb"], 3, 0, 4, -1, 0))
+    assert lib.ph3_tune_set(K["tb"], 3, 0, 4, 99, 0) == 1
+    assert lib.ph3_tune_set(K["tb"], 4, 0, 4, 0, 0) == 1
+    assert lib.ph3_tune_set(K["tb"], 3, 0, 4, 0, -5) == 1

@@ -246,3 +246,29 @@ def test_advance_remainder_rule_and_parity_flag():
 
 def test_device_status_word_is_clear_after_runs():
     assert _lib.device_status(clear=True) == 0
+
+
+@pytest.mark.parametrize("storage", ["float32", "bfloat16"])
+@pytest.mark.parametrize("bc", ["dirichlet", "periodic"])
+def test_every_compiled_config(storage, bc):
+    """Every tile configuration in the tuning table gives the oracle's result."""
+    L = _lib.lib()
+    K = _lib.KERNEL
+    S = _lib.STORAGE[storage]
+    suf = {"float32": "", "bfloat16": "-bf16"}[storage]
+    rng = np.random.default_rng(31)
+    u0 = rng.random((19, 45, 136), dtype=np.float32)
+    st = heat_stencil(3, 0.95 / 6, bc)
+    cases = [("zmarch", 1, "b200/zmarch" + suf)] + [("tb", k, f"b200/tb{k}" + suf)
+                                                      for k in (2, 3, 4, 8)]
+    try:
+        for fam, k, key in cases:
+            for cfg in range(L.ph3_tune_count(K[fam], 3, k)):
+                for chunk in (0, 5):
+                    _lib.check(L.ph3_tune_set(K[fam], 3, S, k, cfg, chunk))
+                    steps = 2 * k + 1
+                    _assert_same(_run(key, u0, st, steps), _ref(key, u0, st, steps),
+                                 (key, cfg, chunk))
+    finally:
+        for fam, k, _ in cases:
+            L.ph3_tune_set(K[fam], 3, S, k, -1, 0)
