@@ -60,6 +60,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--no-variants", action="store_true", help="skip the per-variant table")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--variant", default="b200/zmarch",
+                    help="kernel of the headline line (b200/zmarch; others for profiling)")
     ap.add_argument("--n", type=int, default=N3,
                     help="grid edge of the headline field (512; smaller only for profiling)")
     return ap.parse_args()
@@ -291,7 +293,7 @@ def run_b200(a: argparse.Namespace) -> None:
     cells = u0.size
 
     # ---- value: K solves, field resident in HBM
-    st = make_stepper("b200/zmarch", u0, stencil)
+    st = make_stepper(a.variant, u0, stencil)
     for _ in range(W):
         st.step(T)
     barrier(torch, ws)
@@ -300,10 +302,15 @@ def run_b200(a: argparse.Namespace) -> None:
     barrier(torch, ws)
     secs = max_over_ranks(torch, ws, secs)
     clocks = clk.summary()
-    launches = K * T
+    from pyheat3d_b200.registry import VARIANTS
+
+    var = VARIANTS[a.variant]
+    kpass = var.steps_per_pass
+    launches = K * (T // kpass + T % kpass)
     value = ws * cells * T * K / secs / 1e9
     launch_s = secs / launches
-    alg_bytes = 8.0 * cells  # one fp32 read + one fp32 write per site update
+    # one read + one write of every value per launch (k fused updates per launch for tb<k>)
+    alg_bytes = 2.0 * var.bytes_per_value * cells
     achieved = alg_bytes / launch_s / 1e9
     final_ok = bool(np.isfinite(st.get_tensor().sum().item()))
 
@@ -370,12 +377,12 @@ def run_b200(a: argparse.Namespace) -> None:
         traffic = profile_traffic("zmarch_tma_512cubed_fp32.md")
         line = {
             "metric": "GLUPS (3D 512^3 fp32 periodic FTCS, single-step TMA z-march)",
-            "value": round(value, 2), "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
+            "value": round(value, 2), "kernel": a.variant, "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": round(secs / K * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"3D {a.n}^3 fp32 periodic heat, r=0.95/6, uniform[0,1) "
-                                   "seed 0 (rank r: seed r), b200/zmarch",
-                       "grid": [a.n, a.n, a.n], "bc": "periodic", "storage": "float32",
+            "config": {"workload": f"3D {a.n}^3 {var.storage} periodic heat, r=0.95/6, "
+                                   f"uniform[0,1) seed 0 (rank r: seed r), {a.variant}",
+                       "grid": [a.n, a.n, a.n], "bc": "periodic", "storage": var.storage,
                        "time_steps_per_step": T, "units": "site updates (all cells)",
                        "l2": "inputs larger than L2 (512 MiB field vs 126 MB L2)",
                        "parallelism": f"replicas x{ws}"},

@@ -143,7 +143,9 @@ __device__ __forceinline__ float upd3(float c0, float c1, float ctr, float xm, f
 }
 
 // Packed fp32x2 add / multiply (sm_100a `add.rn.f32x2`, `mul.rn.f32x2`): each lane rounds
-// exactly like __fadd_rn / __fmul_rn, so a packed chain is bit-identical to the scalar one.
+// like __fadd_rn / __fmul_rn. Only additions are chained in packed form: a packed product
+// followed by a packed sum may be contracted into a fused multiply-add by the assembler, so the
+// final c0*u + c1*S uses the scalar non-contracting intrinsics.
 union F2 {
     float2 f;
     unsigned long long u;
@@ -161,16 +163,22 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) {
     return r.f;
 }
 
-// Two neighbouring sites of one row: the same canonical-order update as upd3 / upd2, packed.
+__device__ __forceinline__ float2 lin2(float2 c0, float2 c1, float2 ctr, float2 s) {
+    return make_float2(__fadd_rn(__fmul_rn(c0.x, ctr.x), __fmul_rn(c1.x, s.x)),
+                       __fadd_rn(__fmul_rn(c0.y, ctr.y), __fmul_rn(c1.y, s.y)));
+}
+
+// Two neighbouring sites of one row: the same canonical-order update as upd3 / upd2, with the
+// neighbour sums packed.
 __device__ __forceinline__ float2 upd3_x2(float2 c0, float2 c1, float2 ctr, float2 xm, float2 xp,
                                           float2 ym, float2 yp, float2 zm, float2 zp) {
     const float2 s = add2(add2(add2(xm, xp), add2(ym, yp)), add2(zm, zp));
-    return add2(mul2(c0, ctr), mul2(c1, s));
+    return lin2(c0, c1, ctr, s);
 }
 __device__ __forceinline__ float2 upd2_x2(float2 c0, float2 c1, float2 ctr, float2 xm, float2 xp,
                                           float2 ym, float2 yp) {
     const float2 s = add2(add2(xm, xp), add2(ym, yp));
-    return add2(mul2(c0, ctr), mul2(c1, s));
+    return lin2(c0, c1, ctr, s);
 }
 
 __device__ __forceinline__ int wrap_idx(int i, int n) {

@@ -347,13 +347,23 @@ cudaError_t zmarch_t(const Launch& L) {
     g.nzi = L.periodic ? L.nz : L.nz - 2;
     if (g.nzi <= 0) return cudaSuccess;
     const long long tiles = 1LL * g.ntx * g.nty;
-    // chunk: bounded so that one chunk of the field (read + write) stays well inside L2
+    const long long resident = 1LL * sm_count() * blocks_per_sm[dev];
     int zch = L.chunk;
     if (zch <= 0) {
-        const long long plane_bytes = 1LL * L.nx * L.ny * sizeof(T);
-        const long long cap = std::max(8LL, (32LL << 20) / std::max(1LL, 2 * plane_bytes));
-        zch = int(std::min<long long>(cap, 64));
-        zch = std::min(zch, default_chunk(g.nzi, tiles, 8, 4LL * sm_count() * blocks_per_sm[dev]));
+        if (tiles <= resident) {
+            // one wave: every tile column split into the same number of z-slabs, one slab per
+            // block, all blocks resident. Neighbouring tiles then march through the same planes
+            // at the same time (halo rows come from L2) and each column restarts only at the
+            // slab edges.
+            const long long nslab = std::max(1LL, resident / tiles);
+            zch = int((g.nzi + nslab - 1) / nslab);
+        } else {
+            // more tiles than resident blocks: chunk-major items, a chunk of the field (read +
+            // write) bounded to stay well inside L2
+            const long long plane_bytes = 1LL * L.nx * L.ny * sizeof(T);
+            const long long cap = std::max(8LL, (32LL << 20) / std::max(1LL, 2 * plane_bytes));
+            zch = int(std::min<long long>(cap, 64));
+        }
         zch = std::max(1, std::min(zch, g.nzi));
     }
     g.zch = zch;
@@ -388,10 +398,8 @@ int zmarch_configs(const char** names, int max) {
 
 template <typename T, bool PER>
 static cudaError_t zmarch_cfg(const Launch& L) {
-    // defaults: fp32 -> 16 rows x 8 warps; 16-bit -> 8 rows x 8 warps (one row per warp keeps
-    // the 8-value lanes at low register count)
     int cfg = L.cfg;
-    if (cfg < 0 || cfg >= kZmCount) cfg = sizeof(T) == 4 ? 0 : 1;
+    if (cfg < 0 || cfg >= kZmCount) cfg = 3;  // 16 rows x 16 warps: fastest at 512^3
     switch (cfg) {
         case 0: return zmarch_t<T, PER, 16, 8, 6>(L);
         case 1: return zmarch_t<T, PER, 8, 8, 8>(L);
