@@ -163,9 +163,11 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) {
     return r.f;
 }
 
+// c0*u + c1*S for a pair: packed products, scalar non-contracting sum (checked on the GPU to be
+// bit-identical to the scalar chain; a packed sum of packed products is not).
 __device__ __forceinline__ float2 lin2(float2 c0, float2 c1, float2 ctr, float2 s) {
-    return make_float2(__fadd_rn(__fmul_rn(c0.x, ctr.x), __fmul_rn(c1.x, s.x)),
-                       __fadd_rn(__fmul_rn(c0.y, ctr.y), __fmul_rn(c1.y, s.y)));
+    const float2 a = mul2(c0, ctr), b = mul2(c1, s);
+    return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
 }
 
 // Two neighbouring sites of one row: the same canonical-order update as upd3 / upd2, with the
@@ -173,6 +175,12 @@ __device__ __forceinline__ float2 lin2(float2 c0, float2 c1, float2 ctr, float2 
 __device__ __forceinline__ float2 upd3_x2(float2 c0, float2 c1, float2 ctr, float2 xm, float2 xp,
                                           float2 ym, float2 yp, float2 zm, float2 zp) {
     const float2 s = add2(add2(add2(xm, xp), add2(ym, yp)), add2(zm, zp));
+    return lin2(c0, c1, ctr, s);
+}
+// Same, with the x-neighbour sum (xm + xp) of both sites already formed.
+__device__ __forceinline__ float2 upd3_sx2(float2 c0, float2 c1, float2 ctr, float2 sx, float2 ym,
+                                           float2 yp, float2 zm, float2 zp) {
+    const float2 s = add2(add2(sx, add2(ym, yp)), add2(zm, zp));
     return lin2(c0, c1, ctr, s);
 }
 __device__ __forceinline__ float2 upd2_x2(float2 c0, float2 c1, float2 ctr, float2 xm, float2 xp,

@@ -9,8 +9,8 @@
 //   slowest. The chunk length is chosen on the host to balance the items over the resident
 //   blocks against the 2k warm-up planes every chunk costs.
 // * The level-0 planes of the block's extended tile (EX x EY sites, EX = 32 lanes x V) stream
-//   into a STAGES-deep shared-memory ring with cp.async.bulk row copies (issued by the lanes of
-//   warp 0, one row each) that complete on an mbarrier. A row is one copy, split in two where
+//   into a STAGES-deep shared-memory ring with cp.async.bulk row copies (each warp copies its
+//   own rows) that complete on an mbarrier. A row is one copy, split in two where
 //   it crosses the periodic seam (untiled bulk copies take any 16-byte aligned source address,
 //   so the wrap costs nothing); the ring holds the wrapped extended tile exactly. A stage is
 //   refilled one iteration after it was read: the named barriers of that iteration already
@@ -66,6 +66,29 @@ __device__ __forceinline__ void lds_lane(const T* p, float2 (&v)[V / 2]) {
     for (int q = 0; q < V / 2; ++q) v[q] = make_float2(f[2 * q], f[2 * q + 1]);
 }
 
+// One lane's NP float2 pairs to / from shared memory as a single 8- or 16-byte access
+// (consecutive lanes hit consecutive words: no bank conflicts).
+template <int NP>
+__device__ __forceinline__ void put_lane(float* p, const float2 (&v)[NP]) {
+    if constexpr (NP == 2) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+    } else {
+#pragma unroll
+        for (int q = 0; q < NP; ++q) *reinterpret_cast<float2*>(p + 2 * q) = v[q];
+    }
+}
+template <int NP>
+__device__ __forceinline__ void get_lane(const float* p, float2 (&v)[NP]) {
+    if constexpr (NP == 2) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        v[0] = make_float2(t.x, t.y);
+        v[1] = make_float2(t.z, t.w);
+    } else {
+#pragma unroll
+        for (int q = 0; q < NP; ++q) v[q] = *reinterpret_cast<const float2*>(p + 2 * q);
+    }
+}
+
 template <typename T, int V>
 __device__ __forceinline__ void stg_lane(T* p, const float2 (&v)[V / 2]) {
     float f[V];
@@ -90,16 +113,17 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], NWC);  // one arrival per warp
         fence_mbar_init();
     }
     __syncthreads();
     const int64_t P = int64_t(g.nx) * g.ny;
 
-    // ------------------------------------------------------------------ plane issue (warp 0)
-    // Warp 0 keeps an issue cursor over the same (item, plane) sequence the block consumes and
-    // refills each stage one plane after it was consumed: by then every warp has passed the
-    // named barrier of that iteration, so all reads of the stage are done.
+    // ----------------------------------------------------------------------- plane issue
+    // Every warp keeps an issue cursor over the same (item, plane) sequence the block consumes
+    // and copies its own R rows of each plane (lanes 0..R-1, one row each), announcing their
+    // bytes on the stage's mbarrier. A stage is refilled one plane after it was consumed: by
+    // then every warp has passed the named barriers of that iteration, so all reads are done.
     int is_item = blockIdx.x, is_iz = 0, is_zend = 0;
     uint32_t is_it = 0;
     auto cursor_item = [&](int item) {
@@ -115,10 +139,10 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
         const int xs = tx * OX - KX, ys = ty * OY - K;
         const int s = is_it % STAGES;
         const int pz = PER ? wrap_idx(is_iz, g.nz) : clamp_idx(is_iz, 0, g.nz - 1);
-        if (lane == 0) mbar_arrive_expect_tx(&full[s], C::PLANE_BYTES);
+        if (lane == 0) mbar_arrive_expect_tx(&full[s], R * C::ROW_BYTES);
         __syncwarp();
         T* plane = ring + s * (EY * EX);
-        for (int r = lane; r < EY; r += 32) {
+        for (int r = warp * R + lane; r < warp * R + R && lane < R; r += 32) {
             const int gy = PER ? wrap_idx(ys + r, g.ny) : clamp_idx(ys + r, 0, g.ny - 1);
             const T* row = u + int64_t(pz) * P + int64_t(gy) * g.nx;
             T* dst = plane + r * EX;
@@ -149,10 +173,8 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
             cursor_item(is_item);
         }
     };
-    if (warp == 0) {
-        cursor_item(is_item);
-        for (int i = 0; i < STAGES - 1; ++i) issue_next();
-    }
+    cursor_item(is_item);
+    for (int i = 0; i < STAGES - 1; ++i) issue_next();
 
     // ------------------------------------------------------------------------ all warps
     const float2 c0v = make_float2(c0, c0), c1v = make_float2(c1, c1);
@@ -186,7 +208,7 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 for (int p = 0; p < NP; ++p) A[s][r][p] = B[s][r][p] = make_float2(0.f, 0.f);
 
         for (int iz = z0 - K; iz < z1 + K; ++iz, ++it) {
-            if (warp == 0 && ok) issue_next();
+            if (ok) issue_next();
             const int s = it % STAGES;
             if (ok) {
                 if (mbar_wait(&full[s], (it / STAGES) & 1u, err)) ++waited;
@@ -209,25 +231,21 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 const int c = iz - lev;
                 // y-neighbours of the first / last row: exchange with the adjacent warps
                 float* eb = edge + buf * (2 * NWC * EX);
-                {
-                    float* w0 = eb + warp * EX + lx;
-                    float* w1 = eb + (NWC + warp) * EX + lx;
-#pragma unroll
-                    for (int p = 0; p < NP; ++p) {
-                        *reinterpret_cast<float2*>(w0 + 2 * p) = A[lev - 1][0][p];
-                        *reinterpret_cast<float2*>(w1 + 2 * p) = A[lev - 1][R - 1][p];
-                    }
-                }
+                put_lane<NP>(eb + warp * EX + lx, A[lev - 1][0]);
+                put_lane<NP>(eb + (NWC + warp) * EX + lx, A[lev - 1][R - 1]);
                 named_sync(1, NWC * 32);
                 float2 up[NP], dn[NP];
+                if (warp > 0) {
+                    get_lane<NP>(eb + (NWC + warp - 1) * EX + lx, up);
+                } else {
 #pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                    up[p] = warp > 0 ? *reinterpret_cast<const float2*>(
-                                           eb + (NWC + warp - 1) * EX + lx + 2 * p)
-                                     : A[lev - 1][0][p];
-                    dn[p] = warp < NWC - 1
-                                ? *reinterpret_cast<const float2*>(eb + (warp + 1) * EX + lx + 2 * p)
-                                : A[lev - 1][R - 1][p];
+                    for (int p = 0; p < NP; ++p) up[p] = A[lev - 1][0][p];
+                }
+                if (warp < NWC - 1) {
+                    get_lane<NP>(eb + (warp + 1) * EX + lx, dn);
+                } else {
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) dn[p] = A[lev - 1][R - 1][p];
                 }
                 buf ^= 1;
                 const bool zfix = !PER && (c <= 0 || c >= g.nz - 1);
@@ -297,8 +315,8 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
         }
     }
 
-    // every plane warp 0 issued must land before the block exits (normally all were consumed)
-    if (warp == 0 && lane == 0) {
+    // every plane this warp issued must land before the block exits (normally all were consumed)
+    if (lane == 0) {
         for (uint32_t k = waited; k < is_it; ++k)
             if (!mbar_wait(&full[k % STAGES], (k / STAGES) & 1u, err)) break;
     }
