@@ -44,6 +44,17 @@ int zmarch_configs(const char** names, int max);
 int march_configs(int dims, const char** names, int max);
 int tb_configs(int dims, int k, const char** names, int max);
 
+// FP64 defect-correction kernels and deterministic reductions (ph3_dc.cu). The reductions
+// write kReductionParts partial sums into caller-provided scratch, then sum them in one block.
+constexpr int kReductionParts = 1024;
+cudaError_t launch_dc_residual(int dims, int nz, int ny, int nx, const double* u, const double* f,
+                               double h, float* b, double* out, double* scratch,
+                               cudaStream_t stream);
+cudaError_t launch_dot(const double* x, const double* y, int64_t n, double* out, double* scratch,
+                       cudaStream_t stream);
+cudaError_t launch_dc_correct(double* u, const void* e, int storage, int64_t n,
+                              cudaStream_t stream);
+
 // Number of streaming multiprocessors of the current device (cached per device).
 int sm_count();
 

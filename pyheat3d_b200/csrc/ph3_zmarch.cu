@@ -66,7 +66,7 @@ constexpr int zm_min_blocks() {
     return RW >= 2 ? 1 : 3;
 }
 
-template <typename T, bool PER, int TY, int NWC, int STAGES>
+template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED>
 __global__ void __launch_bounds__(32 * (NWC + 1), zm_min_blocks<T, TY, NWC>())
 zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                   const __grid_constant__ CUtensorMap tm_row,
@@ -253,8 +253,22 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                     const float2 ym = r > 0 ? ctr[r - 1][p] : up[p];
                     float2 yp = dn[p];
                     if (r < RW - 1) yp = r == wrap_r ? wdn[p] : ctr[r + 1][p];
-                    float2 v = upd3_sx2(c0v, c1v, ctr[r][p], sx[p], ym, yp, bel[r][p], abv[r][p]);
-                    if (b != nullptr) v = add2(v, bv[p]);
+                    float2 v;
+                    if constexpr (PACKED) {
+                        v = upd3_sx2(c0v, c1v, ctr[r][p], sx[p], ym, yp, bel[r][p], abv[r][p]);
+                        if (b != nullptr) v = add2(v, bv[p]);
+                    } else {  // scalar chain, same rounding
+                        const float sx0 = __fadd_rn(__fadd_rn(sx[p].x, __fadd_rn(ym.x, yp.x)),
+                                                    __fadd_rn(bel[r][p].x, abv[r][p].x));
+                        const float sx1 = __fadd_rn(__fadd_rn(sx[p].y, __fadd_rn(ym.y, yp.y)),
+                                                    __fadd_rn(bel[r][p].y, abv[r][p].y));
+                        v.x = __fadd_rn(__fmul_rn(c0, ctr[r][p].x), __fmul_rn(c1, sx0));
+                        v.y = __fadd_rn(__fmul_rn(c0, ctr[r][p].y), __fmul_rn(c1, sx1));
+                        if (b != nullptr) {
+                            v.x = __fadd_rn(v.x, bv[p].x);
+                            v.y = __fadd_rn(v.y, bv[p].y);
+                        }
+                    }
                     out[p] = v;
                 }
                 if (!((skipy >> r) & 1u)) {
@@ -335,10 +349,10 @@ bool make_map(CUtensorMap* m, const void* base, int nz, int ny, int nx, int bx, 
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <typename T, bool PER, int TY, int NWC, int STAGES>
+template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED = true>
 cudaError_t zmarch_t(const Launch& L) {
     using C = ZmCfg<T, TY, NWC, STAGES>;
-    auto kern = zmarch_tma_kernel<T, PER, TY, NWC, STAGES>;
+    auto kern = zmarch_tma_kernel<T, PER, TY, NWC, STAGES, PACKED>;
     static int blocks_per_sm[64] = {0};  // per device
     int dev = 0;
     cudaGetDevice(&dev);
@@ -400,8 +414,8 @@ bool zmarch_tma_supported(const Launch& L) {
 
 // Compiled z-march configurations: rows per tile (TY), consumer warps (NWC), ring stages.
 static const char* kZmNames[] = {"TY16_W8_S6", "TY8_W8_S8", "TY32_W8_S4", "TY16_W16_S6",
-                                 "TY8_W4_S8"};
-constexpr int kZmCount = 5;
+                                 "TY8_W4_S8", "TY16_W8_S6_scalar", "TY16_W16_S6_scalar"};
+constexpr int kZmCount = 7;
 
 int zmarch_configs(const char** names, int max) {
     for (int i = 0; i < kZmCount && names != nullptr && i < max; ++i) names[i] = kZmNames[i];
@@ -417,7 +431,9 @@ static cudaError_t zmarch_cfg(const Launch& L) {
         case 1: return zmarch_t<T, PER, 8, 8, 8>(L);
         case 2: return zmarch_t<T, PER, 32, 8, 4>(L);
         case 3: return zmarch_t<T, PER, 16, 16, 6>(L);
-        default: return zmarch_t<T, PER, 8, 4, 8>(L);
+        case 4: return zmarch_t<T, PER, 8, 4, 8>(L);
+        case 5: return zmarch_t<T, PER, 16, 8, 6, false>(L);
+        default: return zmarch_t<T, PER, 16, 16, 6, false>(L);
     }
 }
 

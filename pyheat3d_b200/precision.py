@@ -1,0 +1,163 @@
+"""Mixed-precision Jacobi for lap(u) = f: FP64 defect correction around 16-bit inner sweeps.
+
+The reference solves the Poisson problem with plain Jacobi and the source b = -h^2 f / (2d)
+(pyheat3d ``src/pyheat3d/validation.py:135-147``) in a single precision, which cannot reach a
+1e-10 relative residual in fp32, let alone with 16-bit storage. Here:
+
+* the solution u and the residual r = f - A u live in FP64 on the GPU (``ph3_dc_residual``,
+  ``ph3_dc_correct``: the only FP64 steps);
+* each outer iteration solves the correction equation A e = r approximately with ``m`` Jacobi
+  sweeps on a 16-bit (or fp32) field with fp32 arithmetic — the library's stencil kernels with
+  the source b = -h^2 r / (2d) — starting from e = 0;
+* u <- u + e, and the loop stops when ||r||_2 / ||f||_2 <= tol.
+
+``m`` is chosen from the Jacobi spectral radius rho = cos(pi h) so that one inner solve damps
+the smoothest error mode by the storage type's resolution (``REDUCTION``): reducing further
+gains nothing because e itself is only stored to that precision.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+#: per-outer-iteration damping target of the inner solve, by storage type
+REDUCTION = {"bfloat16": 2.0**-6, "float16": 2.0**-9, "float32": 2.0**-18}
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def inner_sweeps(n: int, storage: str, k: int = 1) -> int:
+    """Jacobi sweeps that damp the smoothest mode by REDUCTION[storage] (multiple of k)."""
+    rho = math.cos(math.pi / (n - 1))
+    m = int(math.ceil(math.log(REDUCTION[storage]) / math.log(rho)))
+    return max(k, int(math.ceil(m / k)) * k)
+
+
+@dataclass
+class DCResult:
+    """Outcome of :meth:`DefectCorrection.solve`."""
+
+    u: object                      # FP64 device tensor (torch)
+    history: list[float]           # relative residual before each outer iteration and at exit
+    outer: int
+    sweeps: int                    # inner Jacobi sweeps in total
+    seconds: float
+    storage: str
+    variant: str
+    converged: bool
+    extra: dict = field(default_factory=dict)
+
+    def host(self) -> np.ndarray:
+        return self.u.cpu().numpy()
+
+
+class DefectCorrection:
+    """FP64 defect correction for lap(u) = f on a Dirichlet grid with zero boundary values.
+
+    ``f``: FP64 array (ny, nx) or (nz, ny, nx) including the boundary layer (ignored there);
+    ``h``: grid spacing; ``storage``: storage type of the inner correction field;
+    ``variant``: "march" (single-step: TMA z-march / y-march) or "tb" with ``k`` steps per pass.
+    """
+
+    def __init__(self, f: np.ndarray, h: float, storage: str = "bfloat16", variant: str = "march",
+                 k: int = 1, device=None):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device")
+        self.lib = _lib.lib()
+        if f.ndim not in (2, 3) or min(f.shape) < 3:
+            raise ValueError("f must be 2D or 3D with at least 3 points per axis")
+        if storage not in _lib.STORAGE:
+            raise ValueError(f"unknown storage {storage!r}")
+        if variant not in ("march", "tb"):
+            raise ValueError("variant must be 'march' or 'tb'")
+        self.dims = f.ndim
+        self.shape = tuple(int(s) for s in f.shape)
+        self.h = float(h)
+        self.storage = storage
+        self.variant = variant
+        self.k = k if variant == "tb" else 1
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        td = getattr(torch, storage)
+        self.f = torch.from_numpy(np.ascontiguousarray(f, dtype=np.float64)).to(self.device)
+        self.u = torch.zeros(self.shape, dtype=torch.float64, device=self.device)
+        self.b = torch.zeros(self.shape, dtype=torch.float32, device=self.device)
+        self.ea = torch.zeros(self.shape, dtype=td, device=self.device)
+        self.eb = torch.zeros(self.shape, dtype=td, device=self.device)
+        self.scratch = torch.empty(int(self.lib.ph3_reduction_scratch_len()),
+                                   dtype=torch.float64, device=self.device)
+        self.rn2 = torch.zeros(1, dtype=torch.float64, device=self.device)
+        core = (slice(1, -1),) * self.dims
+        self.fnorm = float(np.sqrt(np.sum(np.asarray(f, np.float64)[core] ** 2)))
+        if self.dims == 2:
+            self.nz, self.ny, self.nx = 1, self.shape[0], self.shape[1]
+        else:
+            self.nz, self.ny, self.nx = self.shape
+        self.c1 = float(np.float32(1.0 / (2 * self.dims)))
+
+    def _stream(self):
+        return _torch().cuda.current_stream(self.device).cuda_stream
+
+    def residual(self) -> float:
+        """Relative residual ||f - A u|| / ||f|| of the current u (also refreshes b)."""
+        _lib.check(self.lib.ph3_dc_residual(
+            self.dims, self.nz, self.ny, self.nx, self.u.data_ptr(), self.f.data_ptr(), self.h,
+            self.b.data_ptr(), self.rn2.data_ptr(), self.scratch.data_ptr(),
+            self.scratch.numel(), self._stream()))
+        return math.sqrt(max(float(self.rn2.item()), 0.0)) / self.fnorm
+
+    def inner(self, m: int) -> None:
+        """m Jacobi sweeps on A e = r from e = 0, then u += e."""
+        self.ea.zero_()
+        self.eb.zero_()
+        in_b = ctypes.c_int(0)
+        _lib.check(self.lib.ph3_advance(
+            self.dims, self.nz, self.ny, self.nx, _lib.STORAGE[self.storage], _lib.BC["dirichlet"],
+            0.0, self.c1, _lib.VARIANT[self.variant], self.k, self.ea.data_ptr(),
+            self.eb.data_ptr(), self.b.data_ptr(), int(m), self._stream(), ctypes.byref(in_b)))
+        e = self.eb if in_b.value else self.ea
+        _lib.check(self.lib.ph3_dc_correct(self.u.data_ptr(), e.data_ptr(),
+                                           _lib.STORAGE[self.storage], e.numel(),
+                                           self._stream()))
+
+    def solve(self, tol: float = 1e-10, max_outer: int = 60, sweeps: int | list[int] | None = None,
+              check_every: int = 1) -> DCResult:
+        """Outer iterations until the relative residual is <= tol (or max_outer).
+
+        ``sweeps``: inner sweeps per outer iteration (int), an explicit schedule (list; the loop
+        then runs exactly len(schedule) outer iterations), or None for :func:`inner_sweeps`.
+        """
+        torch = _torch()
+        n = min(self.shape)
+        schedule = sweeps if isinstance(sweeps, list) else None
+        m = sweeps if isinstance(sweeps, int) else inner_sweeps(n, self.storage, self.k)
+        torch.cuda.synchronize(self.device)
+        t0 = time.perf_counter()
+        hist = [self.residual()]
+        total = 0
+        outer = 0
+        limit = len(schedule) if schedule is not None else max_outer
+        while outer < limit:
+            if schedule is None and hist[-1] <= tol:
+                break
+            mm = schedule[outer] if schedule is not None else m
+            self.inner(mm)
+            total += mm
+            outer += 1
+            if outer % check_every == 0 or outer == limit:
+                hist.append(self.residual())
+        torch.cuda.synchronize(self.device)
+        secs = time.perf_counter() - t0
+        return DCResult(self.u, hist, outer, total, secs, self.storage,
+                        self.variant if self.k == 1 else f"tb{self.k}", hist[-1] <= tol)
