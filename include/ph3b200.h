@@ -137,6 +137,37 @@ int ph3_dot_f64(const double* x, const double* y, int64_t n, double* out, double
 int ph3_dc_correct(double* u, const void* e, int storage, int64_t n, void* stream);
 
 /*
+ * Batched solves: many independent grids of any sizes advanced in ONE persistent launch (no
+ * counterpart in the reference, which launches every grid and step separately,
+ * cupy_backend.py:183-194). Results equal the single-grid entry points bit for bit.
+ *
+ * Each ph3_problem names a ping-pong pair (a holds the initial state; with PH3_DIRICHLET, b must
+ * hold the same boundary values), the grid, the coefficients and the number of steps. After the
+ * launch a problem's state is in `a` when `steps` is even, else in `b`.
+ *
+ * ph3_batch_workspace_bytes: device workspace (plan + counters) the problem list needs.
+ * ph3_batch_prepare: validate the problems, build the plan and upload it into `ws` (synchronises
+ *   `stream`; not capturable). The problem buffers must stay allocated until the launches end.
+ * ph3_batch_launch: reset the counters and run the persistent kernel on `stream` (capturable in
+ *   a CUDA graph; may be launched again after re-initialising the fields).
+ */
+typedef struct ph3_problem {
+    void* a;
+    void* b;
+    const float* src; /* optional fp32 source b (NULL) */
+    int32_t dims, nz, ny, nx;
+    int32_t bc, storage;
+    float c0, c1;
+    int32_t steps;
+    int32_t reserved; /* must be 0 */
+} ph3_problem;
+
+int64_t ph3_batch_workspace_bytes(const ph3_problem* problems, int n);
+int ph3_batch_prepare(const ph3_problem* problems, int n, void* ws, int64_t ws_bytes,
+                      void* stream);
+int ph3_batch_launch(void* ws, int n, void* stream);
+
+/*
  * Tuning table (no counterpart in the reference, whose tile constants are module globals that
  * bench/tune.py monkey-patches, cupy_backend.py:50-70). Every family has a few compiled tile
  * configurations; the table holds, per (kernel, dims, storage, k), the configuration index and

@@ -327,6 +327,44 @@ int ph3_dc_correct(double* u, const void* e, int storage, int64_t n, void* strea
                   "dc_correct launch");
 }
 
+int64_t ph3_batch_workspace_bytes(const ph3_problem* problems, int n) {
+    if (n < 0 || (n > 0 && problems == nullptr)) {
+        fail(PH3_EINVAL, "problems must be non-null and n >= 0");
+        return -1;
+    }
+    return batch_workspace_bytes(problems, n);
+}
+
+int ph3_batch_prepare(const ph3_problem* problems, int n, void* ws, int64_t ws_bytes,
+                      void* stream) {
+    if (n < 0 || (n > 0 && problems == nullptr) || ws == nullptr)
+        return fail(PH3_EINVAL, "problems and ws must be non-null and n >= 0");
+    for (int i = 0; i < n; ++i) {
+        const ph3_problem& p = problems[i];
+        int rc = check_grid(p.dims, p.dims == 2 ? 1 : p.nz, p.ny, p.nx, p.storage, p.bc);
+        if (rc == PH3_OK) rc = check_ptrs(p.a, p.b, p.src);
+        if (rc != PH3_OK) {
+            char msg[512];
+            snprintf(msg, sizeof(msg), "%s", g_err);
+            return fail(rc, "problem %d: %s", i, msg);
+        }
+        if (p.steps < 0) return fail(PH3_EINVAL, "problem %d: steps must be >= 0", i);
+        if (p.reserved != 0) return fail(PH3_EINVAL, "problem %d: reserved must be 0", i);
+    }
+    const long long need = batch_workspace_bytes(problems, n);
+    if (ws_bytes < need)
+        return fail(PH3_EINVAL, "workspace needs %lld bytes, got %lld", need, (long long)ws_bytes);
+    return finish(batch_prepare(problems, n, ws, ws_bytes, static_cast<cudaStream_t>(stream),
+                                nullptr),
+                  "batch prepare");
+}
+
+int ph3_batch_launch(void* ws, int n, void* stream) {
+    if (ws == nullptr || n < 0) return fail(PH3_EINVAL, "ws must be non-null and n >= 0");
+    return finish(batch_launch(ws, n, status_ptr(), static_cast<cudaStream_t>(stream)),
+                  "batch launch");
+}
+
 static thread_local char g_name[64];
 
 static int check_tune_key(int kernel, int dims, int storage, int k) {

@@ -1,0 +1,286 @@
+// Batched solves: many independent grids of uneven sizes advanced in ONE persistent launch.
+//
+// No counterpart in the reference (one launch per grid and step, cupy_backend.py:183-194). Each
+// problem is cut into tiles (the single-step march tiles of ph3_march.cuh); a work item is
+// (problem P, step s, tile t). Items are numbered round by round — round s holds step s of every
+// problem that still has steps left, problems in descending step count — so every item's
+// predecessors (all tiles of step s-1 of the same problem) come earlier in the numbering.
+// Persistent blocks take items in order from a global counter, wait (bounded) until the
+// problem's step counter reaches s * tiles, run the tile, and count it done. A block only ever
+// waits for items handed out before its own, which are held by running blocks that never wait
+// for later items, so the launch always makes progress.
+//
+// Field reads go through L2 only (__ldcg): other blocks of the same launch write the fields.
+// The item list is implicit: a plan in device memory (problem descriptors, the problems sorted
+// by steps, prefix sums of their tile counts and per-round item offsets) lets a block decode an
+// item number with two binary searches.
+//
+// Workspace layout (caller-allocated device memory, ph3_batch_workspace_bytes):
+//   [counters: u64 next item | i32 abort | i32 pad | i32 done[n]]  (rounded up to 256 bytes)
+//   [header][descriptors][order (i32)][tile prefix (i64)][round offsets (i64)]
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "../../include/ph3b200.h"
+#include "ph3_common.cuh"
+#include "ph3_internal.h"
+#include "ph3_march.cuh"
+
+namespace ph3 {
+
+namespace {
+
+struct BatchDesc {
+    void* a;
+    void* b;
+    const float* src;
+    int dims, nz, ny, nx, periodic, storage;
+    float c0, c1;
+    int steps;
+    int vec;
+    int ntx, nty, ntz, ntiles;
+};
+
+struct BatchHeader {
+    int n;
+    int max_steps;
+    long long total_items;
+    long long off_desc, off_order, off_tilepre, off_round;
+};
+
+constexpr int kW = 8;          // warps per block
+constexpr int kV = 4;          // values per lane (16-bit storage: 8-byte lane vectors)
+constexpr int kR = 2;          // rows per warp (3D tiles)
+constexpr int kZch = 16;       // planes per 3D tile
+constexpr int kRB2 = 2;        // rows per iteration (2D tiles)
+constexpr int kYch = 64;       // rows per 2D tile
+constexpr int kThreads = 32 * kW;
+
+__host__ __device__ __forceinline__ long long counter_bytes(int n) {
+    return ((16LL + 4LL * n + 255) / 256) * 256;
+}
+long long align256(long long x) { return ((x + 255) / 256) * 256; }
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Not inlined: each (storage, boundary) tile body keeps its own register allocation instead of
+// the kernel carrying the union of all six.
+template <typename T, bool PER>
+__device__ __noinline__ void run_tile(const BatchDesc& d, int s, int t, float* edge) {
+    const T* src = static_cast<const T*>((s & 1) ? d.b : d.a);
+    T* dst = static_cast<T*>((s & 1) ? d.a : d.b);
+    if (d.dims == 3) {
+        const int tx = t % d.ntx, ty = (t / d.ntx) % d.nty, tz = t / (d.ntx * d.nty);
+        march3d_item<T, PER, kV, kR, kW, true>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1, tx,
+                                               ty, tz, kZch, d.vec != 0, edge);
+    } else {
+        const int tx = t % d.ntx, ty = t / d.ntx;
+        march2d_item<T, PER, kV, kW, kRB2, true>(src, dst, d.src, d.ny, d.nx, d.c0, d.c1,
+                                                 tx * kW, ty, kYch, d.vec != 0);
+    }
+}
+
+__device__ __forceinline__ long long upper_bound_i64(const long long* a, int n, long long key) {
+    int lo = 0, hi = n;  // first index with a[i] > key
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] <= key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
+    __shared__ __align__(16) float edge[2 * kW * 32 * kV];
+    __shared__ int s_p, s_s, s_t;
+    __shared__ long long s_item;
+    unsigned long long* next = reinterpret_cast<unsigned long long*>(ws);
+    int* abort_flag = reinterpret_cast<int*>(ws + 8);
+    int* done = reinterpret_cast<int*>(ws + 16);
+    const BatchHeader* hd = reinterpret_cast<const BatchHeader*>(ws + counter_bytes(n));
+    const unsigned char* base = reinterpret_cast<const unsigned char*>(hd);
+    const BatchDesc* desc = reinterpret_cast<const BatchDesc*>(base + hd->off_desc);
+    const int* order = reinterpret_cast<const int*>(base + hd->off_order);
+    const long long* tilepre = reinterpret_cast<const long long*>(base + hd->off_tilepre);
+    const long long* round_off = reinterpret_cast<const long long*>(base + hd->off_round);
+    const long long total = hd->total_items;
+    const int max_steps = hd->max_steps;
+
+    for (;;) {
+        if (threadIdx.x == 0) {
+            long long item = static_cast<long long>(atomicAdd(next, 1ULL));
+            if (item >= total || *reinterpret_cast<volatile int*>(abort_flag) != 0) {
+                item = -1;
+            } else {
+                const int s = int(upper_bound_i64(round_off, max_steps + 1, item)) - 1;
+                const long long j = item - round_off[s];
+                const int q = int(upper_bound_i64(tilepre, n + 1, j)) - 1;
+                const int p = order[q];
+                s_p = p;
+                s_s = s;
+                s_t = int(j - tilepre[q]);
+                const int need = s * desc[p].ntiles;
+                uint32_t spins = 0;
+                while (ld_acquire(&done[p]) < need) {
+                    __nanosleep(spins < 64 ? 32 : 256);
+                    if (++spins > kSpinLimit ||
+                        *reinterpret_cast<volatile int*>(abort_flag) != 0) {
+                        record_error(err, kDevDependTimeout);
+                        atomicExch(abort_flag, 1);
+                        item = -1;
+                        break;
+                    }
+                }
+                __threadfence();
+            }
+            s_item = item;
+        }
+        __syncthreads();
+        if (s_item < 0) break;
+        const BatchDesc d = desc[s_p];
+        const int s = s_s, t = s_t;
+        switch (d.storage * 2 + d.periodic) {
+            case 0: run_tile<float, false>(d, s, t, edge); break;
+            case 1: run_tile<float, true>(d, s, t, edge); break;
+            case 2: run_tile<__half, false>(d, s, t, edge); break;
+            case 3: run_tile<__half, true>(d, s, t, edge); break;
+            case 4: run_tile<__nv_bfloat16, false>(d, s, t, edge); break;
+            default: run_tile<__nv_bfloat16, true>(d, s, t, edge); break;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&done[s_p], 1);
+        }
+    }
+}
+
+int blocks_per_sm_cached() {
+    static int nb[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+    if (nb[dev] == 0) {
+        int v = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, batch_kernel, kThreads, 0) !=
+                cudaSuccess ||
+            v < 1)
+            v = 1;
+        nb[dev] = v;
+    }
+    return nb[dev];
+}
+
+int cdiv(long long a, long long b) { return int((a + b - 1) / b); }
+
+// Geometry of one problem's tiles (must match run_tile / the item functions).
+void tiles_of(BatchDesc& d) {
+    const int es = d.storage == kF32 ? 4 : 2;
+    const int EX = 32 * kV;
+    if (d.dims == 3) {
+        d.ntx = cdiv(d.nx, EX);
+        d.nty = cdiv(d.ny, kW * kR);
+        d.ntz = cdiv(d.nz, kZch);
+    } else {
+        d.ntx = cdiv(cdiv(d.nx, EX), kW);
+        d.nty = cdiv(d.ny, kYch);
+        d.ntz = 1;
+    }
+    d.ntiles = d.ntx * d.nty * d.ntz;
+    auto al = [&](const void* p, int bytes) {
+        return p == nullptr || reinterpret_cast<uintptr_t>(p) % bytes == 0;
+    };
+    d.vec = (d.nx % kV == 0) && al(d.a, es * kV) && al(d.b, es * kV) && al(d.src, 4 * kV);
+}
+
+struct Layout {
+    long long cnt, header, desc, order, tilepre, round, total;
+};
+
+Layout layout_of(int n, int max_steps) {
+    Layout L;
+    L.cnt = counter_bytes(n);
+    L.header = L.cnt;
+    L.desc = align256(sizeof(BatchHeader));
+    L.order = L.desc + align256(sizeof(BatchDesc) * (long long)n);
+    L.tilepre = L.order + align256(4LL * n);
+    L.round = L.tilepre + align256(8LL * (n + 1));
+    L.total = L.cnt + L.round + align256(8LL * (max_steps + 1));
+    return L;
+}
+
+}  // namespace
+
+// -------------------------------------------------------------------------------- host API
+long long batch_workspace_bytes(const ph3_problem* p, int n) {
+    int max_steps = 0;
+    for (int i = 0; i < n; ++i) max_steps = std::max(max_steps, p[i].steps);
+    return layout_of(n, max_steps).total;
+}
+
+cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_bytes,
+                          cudaStream_t stream, long long* total_items) {
+    std::vector<BatchDesc> d(n);
+    int max_steps = 0;
+    for (int i = 0; i < n; ++i) {
+        BatchDesc& x = d[i];
+        x.a = p[i].a; x.b = p[i].b; x.src = p[i].src;
+        x.dims = p[i].dims; x.nz = p[i].dims == 2 ? 1 : p[i].nz; x.ny = p[i].ny; x.nx = p[i].nx;
+        x.periodic = p[i].bc == PH3_PERIODIC ? 1 : 0;
+        x.storage = p[i].storage;
+        x.c0 = p[i].c0; x.c1 = p[i].c1;
+        x.steps = p[i].steps;
+        tiles_of(x);
+        max_steps = std::max(max_steps, x.steps);
+    }
+    const Layout L = layout_of(n, max_steps);
+    if (ws_bytes < L.total) return cudaErrorInvalidValue;
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return d[a].steps > d[b].steps; });
+    std::vector<long long> tilepre(n + 1, 0);
+    for (int q = 0; q < n; ++q) tilepre[q + 1] = tilepre[q] + d[order[q]].ntiles;
+    std::vector<long long> round(max_steps + 1, 0);
+    int active = n;
+    for (int s = 0; s < max_steps; ++s) {
+        while (active > 0 && d[order[active - 1]].steps <= s) --active;
+        round[s + 1] = round[s] + tilepre[active];
+    }
+    BatchHeader h;
+    h.n = n;
+    h.max_steps = max_steps;
+    h.total_items = round[max_steps];
+    h.off_desc = L.desc;
+    h.off_order = L.order;
+    h.off_tilepre = L.tilepre;
+    h.off_round = L.round;
+    std::vector<unsigned char> img(L.total - L.header, 0);
+    std::memcpy(img.data(), &h, sizeof(h));
+    std::memcpy(img.data() + L.desc, d.data(), sizeof(BatchDesc) * n);
+    std::memcpy(img.data() + L.order, order.data(), 4 * n);
+    std::memcpy(img.data() + L.tilepre, tilepre.data(), 8 * (n + 1));
+    std::memcpy(img.data() + L.round, round.data(), 8 * (max_steps + 1));
+    cudaError_t e = cudaMemcpyAsync(static_cast<unsigned char*>(ws) + L.header, img.data(),
+                                    img.size(), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(stream);  // the staging image is freed on return
+    if (total_items != nullptr) *total_items = h.total_items;
+    return e;
+}
+
+cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(ws, 0, counter_bytes(n), stream);
+    if (e != cudaSuccess) return e;
+    const int grid = sm_count() * blocks_per_sm_cached();
+    batch_kernel<<<grid, kThreads, 0, stream>>>(static_cast<unsigned char*>(ws), n, err);
+    return cudaGetLastError();
+}
+
+}  // namespace ph3

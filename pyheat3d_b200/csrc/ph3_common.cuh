@@ -34,6 +34,23 @@ template <> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float
 
 template <typename T> __device__ __forceinline__ float ldg1(const T* p) { return to_f(__ldg(p)); }
 
+// Loads that bypass L1 (cache in L2 only): for buffers other blocks of the same launch write,
+// where the read-only path could return stale lines.
+__device__ __forceinline__ float ldcg1(const float* p) { return __ldcg(p); }
+__device__ __forceinline__ float ldcg1(const __half* p) {
+    const unsigned short b = __ldcg(reinterpret_cast<const unsigned short*>(p));
+    return __half2float(__ushort_as_half(b));
+}
+__device__ __forceinline__ float ldcg1(const __nv_bfloat16* p) {
+    const unsigned short b = __ldcg(reinterpret_cast<const unsigned short*>(p));
+    return __uint_as_float(uint32_t(b) << 16);
+}
+// one element through the chosen path (CG: L2 only)
+template <bool CG, typename T> __device__ __forceinline__ float ldx1(const T* p) {
+    if constexpr (CG) return ldcg1(p);
+    else return ldg1(p);
+}
+
 // Vector of V storage elements moved as one 4/8/16-byte access.
 template <typename T, int V> struct VecBits;
 template <typename T> struct VecBits<T, 1> { using type = T; };
@@ -42,15 +59,16 @@ template <> struct VecBytes<4> { using type = uint32_t; };
 template <> struct VecBytes<8> { using type = uint2; };
 template <> struct VecBytes<16> { using type = uint4; };
 
-template <typename T, int V>
+template <typename T, int V, bool CG = false>
 __device__ __forceinline__ void ld_vec(const T* __restrict__ p, float (&v)[V]) {
     constexpr int B = int(sizeof(T)) * V;
     if constexpr (B == 2) {
-        v[0] = to_f(__ldg(p));
+        v[0] = ldx1<CG>(p);
     } else {
         using W = typename VecBytes<B>::type;
         union { W w; T e[V]; } u;
-        u.w = __ldg(reinterpret_cast<const W*>(p));
+        if constexpr (CG) u.w = __ldcg(reinterpret_cast<const W*>(p));
+        else u.w = __ldg(reinterpret_cast<const W*>(p));
 #pragma unroll
         for (int j = 0; j < V; ++j) v[j] = to_f(u.e[j]);
     }

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/ph3b200.h"
+
 namespace ph3 {
 
 enum Storage : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
@@ -54,6 +56,12 @@ cudaError_t launch_dot(const double* x, const double* y, int64_t n, double* out,
                        cudaStream_t stream);
 cudaError_t launch_dc_correct(double* u, const void* e, int storage, int64_t n,
                               cudaStream_t stream);
+
+// Batched persistent launch (ph3_batch.cu).
+long long batch_workspace_bytes(const ph3_problem* p, int n);
+cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_bytes,
+                          cudaStream_t stream, long long* total_items);
+cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream);
 
 // Number of streaming multiprocessors of the current device (cached per device).
 int sm_count();

@@ -11,94 +11,9 @@
 
 #include "ph3_common.cuh"
 #include "ph3_internal.h"
+#include "ph3_march.cuh"
 
 namespace ph3 {
-
-constexpr unsigned kFull = 0xffffffffu;
-
-// ------------------------------------------------------------------------------------------
-// small helpers
-// ------------------------------------------------------------------------------------------
-
-// V fp32 source values starting at p (p aligned to V*4 bytes when vec).
-template <int V>
-__device__ __forceinline__ void ld_src(const float* __restrict__ p, bool vec, float (&v)[V]) {
-    if (vec) {
-        if constexpr (V % 4 == 0) {
-#pragma unroll
-            for (int q = 0; q < V / 4; ++q) {
-                const float4 t = __ldg(reinterpret_cast<const float4*>(p) + q);
-                v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
-            }
-        } else if constexpr (V == 2) {
-            const float2 t = __ldg(reinterpret_cast<const float2*>(p));
-            v[0] = t.x; v[1] = t.y;
-        } else {
-            v[0] = __ldg(p);
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < V; ++j) v[j] = __ldg(p + j);
-    }
-}
-
-template <bool PER>
-__device__ __forceinline__ int fix_idx(int i, int n) {
-    if constexpr (PER) return wrap_idx(i, n);
-    else return clamp_idx(i, 0, n - 1);
-}
-
-// Column addressing of one thread's V consecutive x-values starting at gx.
-// vec: the V values are one aligned vector (nx % V == 0 and gx % V == 0), addressed by `base`.
-// scalar: each value has its own wrapped / clamped column in cx[].
-template <bool PER, int V>
-struct Cols {
-    int base;
-    int cx[V];
-    __device__ __forceinline__ void init(int gx, int nx, bool vec) {
-        if (vec) {
-            base = PER ? wrap_idx(gx, nx) : clamp_idx(gx, 0, nx - V);
-#pragma unroll
-            for (int j = 0; j < V; ++j) cx[j] = base + j;
-        } else {
-            base = 0;
-#pragma unroll
-            for (int j = 0; j < V; ++j) cx[j] = fix_idx<PER>(gx + j, nx);
-        }
-    }
-    template <typename T>
-    __device__ __forceinline__ void load(const T* __restrict__ row, bool vec, float (&v)[V]) const {
-        if (vec) {
-            ld_vec<T, V>(row + base, v);
-        } else {
-#pragma unroll
-            for (int j = 0; j < V; ++j) v[j] = ldg1(row + cx[j]);
-        }
-    }
-    __device__ __forceinline__ void load_src(const float* __restrict__ row, bool vec,
-                                             float (&v)[V]) const {
-        if (vec) {
-            ld_src<V>(row + base, true, v);
-        } else {
-#pragma unroll
-            for (int j = 0; j < V; ++j) v[j] = __ldg(row + cx[j]);
-        }
-    }
-};
-
-// Store V values at columns gx..gx+V-1 of `row` (unwrapped; only in-domain columns written).
-// `skip` has bit j set for columns that must not be written (Dirichlet boundary).
-template <typename T, int V>
-__device__ __forceinline__ void store_cols(T* __restrict__ row, int gx, int nx, bool vec,
-                                           uint32_t skip, const float (&v)[V]) {
-    if (vec && skip == 0 && gx + V <= nx) {
-        st_vec<T, V>(row + gx, v);
-        return;
-    }
-#pragma unroll
-    for (int j = 0; j < V; ++j)
-        if (gx + j < nx && !((skip >> j) & 1u)) row[gx + j] = from_f<T>(v[j]);
-}
 
 // ------------------------------------------------------------------------------------------
 // naive: one lattice site per thread; every operand through L1/L2
@@ -153,211 +68,21 @@ naive3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restri
     o[c + i] = from_f<T>(v);
 }
 
-// ------------------------------------------------------------------------------------------
-// 2D single step, y-march: warp w of the block owns a strip of 32*V columns (lane l holds
-// columns x0 + l*V .. +V-1 as one vector) and walks a chunk of rows, RB rows per iteration, with
-// the next RB rows already in flight. x-neighbours come from warp shuffles (lanes 0 and 31 load
-// the strip's halo columns), y-neighbours from the row window in registers. No shared memory.
-// ------------------------------------------------------------------------------------------
 template <typename T, bool PER, int V, int W, int RB>
 __global__ void __launch_bounds__(32 * W)
 march2d_k1_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b,
                   int ny, int nx, float c0, float c1, int ych, int vec_i) {
-    constexpr int EX = 32 * V;
-    const bool vec = vec_i != 0;
-    const int lane = threadIdx.x & 31;
-    const int strip = blockIdx.x * W + (threadIdx.x >> 5);
-    const int x0 = strip * EX;
-    if (x0 >= nx) return;  // whole warp leaves together; no block-wide sync in this kernel
-    const int gx = x0 + lane * V;
-    int ylo = blockIdx.y * ych, yhi = min(ylo + ych, ny);
-    if constexpr (!PER) { ylo = max(ylo, 1); yhi = min(yhi, ny - 1); }
-    if (ylo >= yhi) return;
-
-    Cols<PER, V> cols;
-    cols.init(gx, nx, vec);
-    const int xl = fix_idx<PER>(x0 - 1, nx);
-    const int xr = fix_idx<PER>(x0 + EX, nx);
-    uint32_t skip = 0;  // Dirichlet boundary / outside columns are never written
-    if constexpr (!PER) {
-#pragma unroll
-        for (int j = 0; j < V; ++j)
-            if (gx + j <= 0 || gx + j >= nx - 1) skip |= 1u << j;
-    }
-
-    // window rows ylo-1 .. ylo+RB (RB + 2 rows), halos per row, prefetch RB rows
-    float win[RB + 2][V], hl[RB + 2], hr[RB + 2];
-    float pre[RB][V], pl[RB], pr[RB];
-    auto load_row = [&](int y, float (&v)[V], float& l, float& r) {
-        const T* row = u + int64_t(fix_idx<PER>(y, ny)) * nx;
-        cols.load(row, vec, v);
-        l = lane == 0 ? ldg1(row + xl) : 0.f;
-        r = lane == 31 ? ldg1(row + xr) : 0.f;
-    };
-#pragma unroll
-    for (int q = 0; q < RB + 2; ++q) load_row(ylo - 1 + q, win[q], hl[q], hr[q]);
-
-    for (int y = ylo; y < yhi; y += RB) {
-        const bool more = y + RB < yhi;
-        if (more) {
-#pragma unroll
-            for (int q = 0; q < RB; ++q) load_row(y + RB + 1 + q, pre[q], pl[q], pr[q]);
-        }
-#pragma unroll
-        for (int q = 0; q < RB; ++q) {
-            const int yy = y + q;
-            if (yy >= yhi) break;
-            float out[V];
-            const float left = __shfl_up_sync(kFull, win[q + 1][V - 1], 1);
-            const float right = __shfl_down_sync(kFull, win[q + 1][0], 1);
-            float bv[V];
-            if (b != nullptr) cols.load_src(b + int64_t(yy) * nx, vec, bv);
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-                const float xm = j > 0 ? win[q + 1][j - 1] : (lane == 0 ? hl[q + 1] : left);
-                const float xp = j < V - 1 ? win[q + 1][j + 1] : (lane == 31 ? hr[q + 1] : right);
-                float v = upd2(c0, c1, win[q + 1][j], xm, xp, win[q][j], win[q + 2][j]);
-                if (b != nullptr) v = __fadd_rn(v, bv[j]);
-                out[j] = v;
-            }
-            store_cols<T, V>(o + int64_t(yy) * nx, gx, nx, vec, skip, out);
-        }
-        if (more) {
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-                win[0][j] = win[RB][j];
-                win[1][j] = win[RB + 1][j];
-            }
-            hl[0] = hl[RB]; hl[1] = hl[RB + 1]; hr[0] = hr[RB]; hr[1] = hr[RB + 1];
-#pragma unroll
-            for (int q = 0; q < RB; ++q) {
-#pragma unroll
-                for (int j = 0; j < V; ++j) win[q + 2][j] = pre[q][j];
-                hl[q + 2] = pl[q];
-                hr[q + 2] = pr[q];
-            }
-        }
-    }
+    march2d_item<T, PER, V, W, RB, false>(u, o, b, ny, nx, c0, c1, blockIdx.x * W, blockIdx.y,
+                                          ych, vec_i != 0);
 }
 
-// ------------------------------------------------------------------------------------------
-// 3D single step, z-march with plain loads (any shape): the block owns an xy tile of 32*V x
-// W*R sites; warp w holds R rows, lane l holds V columns per row as one vector. The z-neighbours
-// form a register queue (below / centre / above) and the plane after `above` is in flight while
-// a plane is computed. x-neighbours: shuffles (+ halo columns loaded by lanes 0 and 31);
-// y-neighbours: own registers, the first/last rows of the neighbouring warps through shared
-// memory, and the tile's halo rows loaded by the first and last warp.
-// ------------------------------------------------------------------------------------------
 template <typename T, bool PER, int V, int R, int W>
 __global__ void __launch_bounds__(32 * W)
 march3d_k1_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b,
                   int nz, int ny, int nx, float c0, float c1, int zch, int vec_i) {
-    constexpr int EX = 32 * V, EY = W * R;
-    __shared__ __align__(16) float edge[2][W][EX];  // [first/last row][warp][column]
-    const bool vec = vec_i != 0;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int x0 = blockIdx.x * EX, y0 = blockIdx.y * EY;
-    const int gx = x0 + lane * V, gy0 = y0 + w * R;
-    int zlo = blockIdx.z * zch, zhi = min(zlo + zch, nz);
-    if constexpr (!PER) { zlo = max(zlo, 1); zhi = min(zhi, nz - 1); }
-    if (zlo >= zhi) return;  // uniform over the block
-
-    const int64_t P = int64_t(nx) * ny;
-    Cols<PER, V> cols;
-    cols.init(gx, nx, vec);
-    int64_t roff[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) roff[r] = int64_t(fix_idx<PER>(gy0 + r, ny)) * nx;
-    const int64_t rtop = int64_t(fix_idx<PER>(y0 - 1, ny)) * nx;
-    const int64_t rbot = int64_t(fix_idx<PER>(y0 + EY, ny)) * nx;
-    const int xl = fix_idx<PER>(x0 - 1, nx), xr = fix_idx<PER>(x0 + EX, nx);
-    uint32_t skipx = 0, skipy = 0;
-    if constexpr (!PER) {
-#pragma unroll
-        for (int j = 0; j < V; ++j)
-            if (gx + j <= 0 || gx + j >= nx - 1) skipx |= 1u << j;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (gy0 + r <= 0 || gy0 + r >= ny - 1) skipy |= 1u << r;
-    }
-
-    struct Plane {
-        float v[R][V];
-        float l[R], r[R];    // halo columns (lanes 0 / 31)
-        float t[V], bt[V];   // halo rows (warp 0 / warp W-1)
-    };
-    auto load_plane = [&](int z, Plane& p) {
-        const T* pl = u + int64_t(fix_idx<PER>(z, nz)) * P;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            cols.load(pl + roff[r], vec, p.v[r]);
-            p.l[r] = lane == 0 ? ldg1(pl + roff[r] + xl) : 0.f;
-            p.r[r] = lane == 31 ? ldg1(pl + roff[r] + xr) : 0.f;
-        }
-        if (w == 0) cols.load(pl + rtop, vec, p.t);
-        if (w == W - 1) cols.load(pl + rbot, vec, p.bt);
-    };
-
-    float bel[R][V];
-    Plane ctr, abv, pre;
-    {
-        const T* pl = u + int64_t(fix_idx<PER>(zlo - 1, nz)) * P;
-#pragma unroll
-        for (int r = 0; r < R; ++r) cols.load(pl + roff[r], vec, bel[r]);
-    }
-    load_plane(zlo, ctr);
-    load_plane(zlo + 1, abv);
-
-    for (int z = zlo; z < zhi; ++z) {
-        const bool more = z + 1 < zhi;
-        if (more) load_plane(z + 2, pre);
-        // y-neighbours across warps
-        float up[V], dn[V];
-        if constexpr (W > 1) {
-            __syncthreads();  // previous iteration's reads of edge[] are done
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-                edge[0][w][lane * V + j] = ctr.v[0][j];
-                edge[1][w][lane * V + j] = ctr.v[R - 1][j];
-            }
-            __syncthreads();
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-                up[j] = w > 0 ? edge[1][w - 1][lane * V + j] : ctr.t[j];
-                dn[j] = w < W - 1 ? edge[0][w + 1][lane * V + j] : ctr.bt[j];
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < V; ++j) { up[j] = ctr.t[j]; dn[j] = ctr.bt[j]; }
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const float left = __shfl_up_sync(kFull, ctr.v[r][V - 1], 1);
-            const float right = __shfl_down_sync(kFull, ctr.v[r][0], 1);
-            float bv[V];
-            if (b != nullptr) cols.load_src(b + int64_t(z) * P + roff[r], vec, bv);
-            float out[V];
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-                const float xm = j > 0 ? ctr.v[r][j - 1] : (lane == 0 ? ctr.l[r] : left);
-                const float xp = j < V - 1 ? ctr.v[r][j + 1] : (lane == 31 ? ctr.r[r] : right);
-                const float ym = r > 0 ? ctr.v[r - 1][j] : up[j];
-                const float yp = r < R - 1 ? ctr.v[r + 1][j] : dn[j];
-                float v = upd3(c0, c1, ctr.v[r][j], xm, xp, ym, yp, bel[r][j], abv.v[r][j]);
-                if (b != nullptr) v = __fadd_rn(v, bv[j]);
-                out[j] = v;
-            }
-            const int gy = gy0 + r;
-            if (gy < ny && !((skipy >> r) & 1u))
-                store_cols<T, V>(o + int64_t(z) * P + int64_t(gy) * nx, gx, nx, vec, skipx, out);
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-            for (int j = 0; j < V; ++j) bel[r][j] = ctr.v[r][j];
-        ctr = abv;
-        if (more) abv = pre;
-    }
+    __shared__ __align__(16) float edge[2 * W * 32 * V];
+    march3d_item<T, PER, V, R, W, false>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x, blockIdx.y,
+                                         blockIdx.z, zch, vec_i != 0, edge);
 }
 
 // ------------------------------------------------------------------------------------------
