@@ -122,19 +122,22 @@ int ph3_advance(int dims, int nz, int ny, int nx, int storage, int bc, float c0,
  *
  * ph3_reduction_scratch_len: doubles of scratch the reductions below need (a constant).
  * ph3_dc_residual: FP64 residual r = f - A u, A u = (S(u) - 2d u) / h^2 on the interior
- *   (r = 0 on the boundary layer), written as the fp32 Jacobi source b = -h^2 r / (2d) of the
- *   correction equation A e = r (b may be NULL), and *rnorm2 = sum(r^2) (a device pointer).
- *   u, f: FP64 arrays of the grid's shape; nz = 1 in 2D.
+ *   (r = 0 on the boundary layer), written as the fp32 Jacobi source
+ *   b = ((-h^2 / (2d)) * b_scale) * r of the scaled correction equation A e = b_scale * r
+ *   (b may be NULL; b_scale is normally 1/s for a power of two s), and *rnorm2 = sum(r^2)
+ *   (a device pointer). u, f: FP64 arrays of the grid's shape; nz = 1 in 2D.
  * ph3_dot_f64: *out = sum(x * y) over n FP64 values (device pointer out).
- * ph3_dc_correct: u += e over n values; u FP64, e in `storage` (the correction).
+ * ph3_dc_correct: u += e_scale * e over n values; u FP64, e in `storage` (the correction).
  * Sums are deterministic for a given input (fixed partition and summation order).
  */
 int64_t ph3_reduction_scratch_len(void);
 int ph3_dc_residual(int dims, int nz, int ny, int nx, const double* u, const double* f, double h,
-                    float* b, double* rnorm2, double* scratch, int64_t scratch_len, void* stream);
+                    double b_scale, float* b, double* rnorm2, double* scratch, int64_t scratch_len,
+                    void* stream);
 int ph3_dot_f64(const double* x, const double* y, int64_t n, double* out, double* scratch,
                 int64_t scratch_len, void* stream);
-int ph3_dc_correct(double* u, const void* e, int storage, int64_t n, void* stream);
+int ph3_dc_correct(double* u, const void* e, int storage, double e_scale, int64_t n,
+                   void* stream);
 
 /*
  * Batched solves: many independent grids of any sizes advanced in ONE persistent launch (no

@@ -7,8 +7,10 @@ module states, operation by operation, what the GPU computes, so small cases mat
 
 - :func:`residual_f64` — r = f - A u with A u = (S(u) - 2d u) / h^2 (S in the canonical x, y, z
   order), r = 0 on the boundary, b = float32(-h^2 r / (2d)), and sum(r^2);
-- :func:`defect_correction` — the outer loop with the inner Jacobi sweeps emulated by
-  :func:`oracle.stencil.emulated_reference` (16-bit storage rounding, source b added last);
+- :func:`defect_correction` — the outer loop: a power-of-two scale s near the residual's RMS,
+  the scaled correction equation A e = r / s solved by Jacobi sweeps emulated by
+  :func:`oracle.stencil.emulated_reference` (16-bit storage rounding, source b added last), and
+  u <- u + s e;
 - :func:`manufactured` / :func:`discrete_solution` — the manufactured problem and its exact
   discrete (FP64) solution: f is an eigenfunction of the discrete Laplacian, so the converged
   FP64 Jacobi iterate is known in closed form.
@@ -56,7 +58,15 @@ def discrete_solution(n: int, dims: int) -> np.ndarray:
     return f / lam
 
 
-def residual_f64(u: np.ndarray, f: np.ndarray, h: float):
+def pow2_scale(rn2: float, ncells: int) -> float:
+    """Power of two at or below the residual's RMS (1.0 for a zero residual)."""
+    rms = math.sqrt(rn2 / max(ncells, 1))
+    if not rms > 0.0 or not math.isfinite(rms):
+        return 1.0
+    return math.ldexp(1.0, math.floor(math.log2(rms)))
+
+
+def residual_f64(u: np.ndarray, f: np.ndarray, h: float, b_scale: float = 1.0):
     """(r, b, sum(r^2)) exactly as the GPU's FP64 residual kernel computes r and b."""
     d = u.ndim
     core = (slice(1, -1),) * d
@@ -69,7 +79,7 @@ def residual_f64(u: np.ndarray, f: np.ndarray, h: float):
     au = (s - (2.0 * d) * u[core]) * inv_h2
     r = np.zeros_like(u)
     r[core] = f[core] - au
-    bscale = -(h * h) / (2.0 * d)
+    bscale = (-(h * h) / (2.0 * d)) * b_scale
     b = (bscale * r).astype(np.float32)
     return r, b, float(np.sum(r * r))
 
@@ -86,12 +96,15 @@ def defect_correction(f: np.ndarray, h: float, storage: str, k: int, sweeps: lis
     u = np.zeros_like(f, dtype=np.float64)
     fn = math.sqrt(float(np.sum(f[(slice(1, -1),) * d] ** 2)))
     hist = []
+    ncore = int(np.prod([s - 2 for s in f.shape]))
     for m in sweeps:
-        _, b, rn2 = residual_f64(u, f, h)
+        _, _, rn2 = residual_f64(u, f, h)
         hist.append(math.sqrt(rn2) / fn)
+        sc = pow2_scale(rn2, ncore)
+        _, b, _ = residual_f64(u, f, h, 1.0 / sc)
         e = emulated_reference(np.zeros(f.shape, np.float32), c0, c1, "dirichlet", m, storage,
                                k, b)
-        u = u + e.astype(np.float64)
+        u = u + sc * e.astype(np.float64)
     _, _, rn2 = residual_f64(u, f, h)
     hist.append(math.sqrt(rn2) / fn)
     return u, hist

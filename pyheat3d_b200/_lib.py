@@ -32,9 +32,13 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "ph3_advance": (_i, [_i, _i, _i, _i, _i, _i, _f, _f, _i, _i, _p, _p, _p, _i64, _p,
                          ctypes.POINTER(_i)]),
     "ph3_reduction_scratch_len": (_i64, []),
-    "ph3_dc_residual": (_i, [_i, _i, _i, _i, _p, _p, ctypes.c_double, _p, _p, _p, _i64, _p]),
+    "ph3_dc_residual": (_i, [_i, _i, _i, _i, _p, _p, ctypes.c_double, ctypes.c_double, _p, _p,
+                             _p, _i64, _p]),
     "ph3_dot_f64": (_i, [_p, _p, _i64, _p, _p, _i64, _p]),
-    "ph3_dc_correct": (_i, [_p, _p, _i, _i64, _p]),
+    "ph3_dc_correct": (_i, [_p, _p, _i, ctypes.c_double, _i64, _p]),
+    "ph3_batch_workspace_bytes": (_i64, [_p, _i]),
+    "ph3_batch_prepare": (_i, [_p, _i, _p, _i64, _p]),
+    "ph3_batch_launch": (_i, [_p, _i, _p]),
     "ph3_tune_count": (_i, [_i, _i, _i]),
     "ph3_tune_name": (ctypes.c_char_p, [_i, _i, _i, _i]),
     "ph3_tune_set": (_i, [_i, _i, _i, _i, _i, _i]),

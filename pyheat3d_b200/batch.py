@@ -41,24 +41,6 @@ class ProblemDesc(ctypes.Structure):
                 ("reserved", ctypes.c_int32)]
 
 
-_BOUND = False
-
-
-def _bind(L) -> None:
-    global _BOUND
-    if _BOUND:
-        return
-    P = ctypes.POINTER(ProblemDesc)
-    L.ph3_batch_workspace_bytes.restype = ctypes.c_int64
-    L.ph3_batch_workspace_bytes.argtypes = [P, ctypes.c_int]
-    L.ph3_batch_prepare.restype = ctypes.c_int
-    L.ph3_batch_prepare.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
-                                    ctypes.c_void_p]
-    L.ph3_batch_launch.restype = ctypes.c_int
-    L.ph3_batch_launch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
-    _BOUND = True
-
-
 @dataclass
 class Problem:
     """One grid: initial state, coefficients (``stencil`` with c0, c1, bc), steps, storage."""
@@ -85,7 +67,6 @@ class Batch:
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device")
         self.lib = _lib.lib()
-        _bind(self.lib)
         self.device = device or torch.device("cuda", torch.cuda.current_device())
         self.problems = list(problems)
         n = len(self.problems)
@@ -116,11 +97,12 @@ class Batch:
             d.steps = int(p.steps)
             d.reserved = 0
         self.n = n
-        nbytes = int(self.lib.ph3_batch_workspace_bytes(self.descs, n))
+        descs = ctypes.addressof(self.descs)
+        nbytes = int(self.lib.ph3_batch_workspace_bytes(descs, n))
         if nbytes < 0:
             _lib.check(1)
         self.ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
-        _lib.check(self.lib.ph3_batch_prepare(self.descs, n, self.ws.data_ptr(), self.ws.numel(),
+        _lib.check(self.lib.ph3_batch_prepare(descs, n, self.ws.data_ptr(), self.ws.numel(),
                                               self._stream()))
 
     def _stream(self):

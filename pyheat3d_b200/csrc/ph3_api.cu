@@ -291,8 +291,8 @@ int ph3_advance(int dims, int nz, int ny, int nx, int storage, int bc, float c0,
 int64_t ph3_reduction_scratch_len(void) { return kReductionParts; }
 
 int ph3_dc_residual(int dims, int nz, int ny, int nx, const double* u, const double* f, double h,
-                    float* b, double* rnorm2, double* scratch, int64_t scratch_len,
-                    void* stream) {
+                    double b_scale, float* b, double* rnorm2, double* scratch,
+                    int64_t scratch_len, void* stream) {
     int rc = check_grid(dims, dims == 2 ? 1 : nz, ny, nx, PH3_FLOAT32, PH3_DIRICHLET);
     if (rc != PH3_OK) return rc;
     if (u == nullptr || f == nullptr || rnorm2 == nullptr || scratch == nullptr)
@@ -301,7 +301,7 @@ int ph3_dc_residual(int dims, int nz, int ny, int nx, const double* u, const dou
         return fail(PH3_EINVAL, "scratch needs %d doubles, got %lld", kReductionParts,
                     (long long)scratch_len);
     if (!(h > 0.0)) return fail(PH3_EINVAL, "h must be > 0");
-    return finish(launch_dc_residual(dims, nz, ny, nx, u, f, h, b, rnorm2, scratch,
+    return finish(launch_dc_residual(dims, nz, ny, nx, u, f, h, b_scale, b, rnorm2, scratch,
                                      static_cast<cudaStream_t>(stream)),
                   "dc_residual launch");
 }
@@ -318,12 +318,13 @@ int ph3_dot_f64(const double* x, const double* y, int64_t n, double* out, double
                   "dot launch");
 }
 
-int ph3_dc_correct(double* u, const void* e, int storage, int64_t n, void* stream) {
+int ph3_dc_correct(double* u, const void* e, int storage, double e_scale, int64_t n,
+                   void* stream) {
     if (u == nullptr || e == nullptr) return fail(PH3_EINVAL, "u and e must be non-null");
     if (storage < PH3_FLOAT32 || storage > PH3_BFLOAT16)
         return fail(PH3_EINVAL, "storage must be 0, 1 or 2, got %d", storage);
     if (n < 0) return fail(PH3_EINVAL, "n must be >= 0");
-    return finish(launch_dc_correct(u, e, storage, n, static_cast<cudaStream_t>(stream)),
+    return finish(launch_dc_correct(u, e, storage, e_scale, n, static_cast<cudaStream_t>(stream)),
                   "dc_correct launch");
 }
 

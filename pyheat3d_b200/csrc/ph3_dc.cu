@@ -7,9 +7,12 @@
 // 16-bit storage and fp32 arithmetic (the stencil kernels of this library, with a source):
 //
 //   r = f - A u,        A u = (S(u) - 2d u) / h^2      (FP64, interior; r = 0 on the boundary)
-//   b = -h^2 r / (2d)   (fp32 source of the correction equation A e = r)
+//   b = -h^2 (r / s) / (2d)   (fp32 source of the scaled correction equation A e = r / s)
 //   e <- Jacobi sweeps (16-bit storage, fp32 math, e = 0 on the boundary)
-//   u <- u + e          (FP64)
+//   u <- u + s e        (FP64)
+// The scale s is a power of two near the residual's RMS, chosen by the host, so the correction
+// stays inside the 16-bit exponent range (fp16 would otherwise flush it to zero) and scaling is
+// exact.
 //
 // Every FP64 operation is an explicitly rounded __dadd_rn / __dmul_rn in a fixed order, so the
 // NumPy oracle reproduces residual and update bit for bit. Reductions are two-pass and
@@ -87,19 +90,20 @@ finish_kernel(const double* __restrict__ partial, int nparts, double* __restrict
 }
 
 template <typename T>
-__global__ void correct_kernel(double* __restrict__ u, const T* __restrict__ e, int64_t n) {
+__global__ void correct_kernel(double* __restrict__ u, const T* __restrict__ e, double scale,
+                               int64_t n) {
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += int64_t(gridDim.x) * blockDim.x)
-        u[i] = __dadd_rn(u[i], double(to_f(e[i])));
+        u[i] = __dadd_rn(u[i], __dmul_rn(scale, double(to_f(e[i]))));
 }
 
 }  // namespace
 
 cudaError_t launch_dc_residual(int dims, int nz, int ny, int nx, const double* u, const double* f,
-                               double h, float* b, double* out, double* scratch,
+                               double h, double b_scale, float* b, double* out, double* scratch,
                                cudaStream_t stream) {
     const double inv_h2 = 1.0 / (h * h);
-    const double bscale = -(h * h) / (2.0 * dims);
+    const double bscale = (-(h * h) / (2.0 * dims)) * b_scale;
     if (dims == 3)
         dc_residual_kernel<3><<<kReductionParts, kRedThreads, 0, stream>>>(
             u, f, nz, ny, nx, inv_h2, bscale, b, scratch);
@@ -121,18 +125,19 @@ cudaError_t launch_dot(const double* x, const double* y, int64_t n, double* out,
     return cudaGetLastError();
 }
 
-cudaError_t launch_dc_correct(double* u, const void* e, int storage, int64_t n,
+cudaError_t launch_dc_correct(double* u, const void* e, int storage, double scale, int64_t n,
                               cudaStream_t stream) {
     const int blocks = 4 * (sm_count() > 0 ? sm_count() : 148);
     switch (storage) {
         case kF32:
-            correct_kernel<<<blocks, 256, 0, stream>>>(u, static_cast<const float*>(e), n);
+            correct_kernel<<<blocks, 256, 0, stream>>>(u, static_cast<const float*>(e), scale, n);
             break;
         case kF16:
-            correct_kernel<<<blocks, 256, 0, stream>>>(u, static_cast<const __half*>(e), n);
+            correct_kernel<<<blocks, 256, 0, stream>>>(u, static_cast<const __half*>(e), scale, n);
             break;
         case kBF16:
-            correct_kernel<<<blocks, 256, 0, stream>>>(u, static_cast<const __nv_bfloat16*>(e), n);
+            correct_kernel<<<blocks, 256, 0, stream>>>(u, static_cast<const __nv_bfloat16*>(e),
+                                                      scale, n);
             break;
         default: return cudaErrorInvalidValue;
     }

@@ -50,11 +50,11 @@ int tb_configs(int dims, int k, const char** names, int max);
 // write kReductionParts partial sums into caller-provided scratch, then sum them in one block.
 constexpr int kReductionParts = 1024;
 cudaError_t launch_dc_residual(int dims, int nz, int ny, int nx, const double* u, const double* f,
-                               double h, float* b, double* out, double* scratch,
+                               double h, double b_scale, float* b, double* out, double* scratch,
                                cudaStream_t stream);
 cudaError_t launch_dot(const double* x, const double* y, int64_t n, double* out, double* scratch,
                        cudaStream_t stream);
-cudaError_t launch_dc_correct(double* u, const void* e, int storage, int64_t n,
+cudaError_t launch_dc_correct(double* u, const void* e, int storage, double scale, int64_t n,
                               cudaStream_t stream);
 
 // Batched persistent launch (ph3_batch.cu).

@@ -6,10 +6,11 @@ The reference solves the Poisson problem with plain Jacobi and the source b = -h
 
 * the solution u and the residual r = f - A u live in FP64 on the GPU (``ph3_dc_residual``,
   ``ph3_dc_correct``: the only FP64 steps);
-* each outer iteration solves the correction equation A e = r approximately with ``m`` Jacobi
-  sweeps on a 16-bit (or fp32) field with fp32 arithmetic — the library's stencil kernels with
-  the source b = -h^2 r / (2d) — starting from e = 0;
-* u <- u + e, and the loop stops when ||r||_2 / ||f||_2 <= tol.
+* each outer iteration solves the scaled correction equation A e = r / s (s: a power of two at
+  or below the residual's RMS, so e stays inside the 16-bit exponent range) approximately with
+  ``m`` Jacobi sweeps on a 16-bit (or fp32) field with fp32 arithmetic — the library's stencil
+  kernels with the source b = -h^2 (r / s) / (2d) — starting from e = 0;
+* u <- u + s e, and the loop stops when ||r||_2 / ||f||_2 <= tol.
 
 ``m`` is chosen from the Jacobi spectral radius rho = cos(pi h) so that one inner solve damps
 the smoothest error mode by the storage type's resolution (``REDUCTION``): reducing further
@@ -109,16 +110,29 @@ class DefectCorrection:
     def _stream(self):
         return _torch().cuda.current_stream(self.device).cuda_stream
 
-    def residual(self) -> float:
-        """Relative residual ||f - A u|| / ||f|| of the current u (also refreshes b)."""
+    def _residual(self, b_scale: float, with_b: bool) -> float:
         _lib.check(self.lib.ph3_dc_residual(
             self.dims, self.nz, self.ny, self.nx, self.u.data_ptr(), self.f.data_ptr(), self.h,
-            self.b.data_ptr(), self.rn2.data_ptr(), self.scratch.data_ptr(),
-            self.scratch.numel(), self._stream()))
-        return math.sqrt(max(float(self.rn2.item()), 0.0)) / self.fnorm
+            b_scale, self.b.data_ptr() if with_b else None, self.rn2.data_ptr(),
+            self.scratch.data_ptr(), self.scratch.numel(), self._stream()))
+        return max(float(self.rn2.item()), 0.0)
+
+    def residual(self) -> float:
+        """Relative residual ||f - A u|| / ||f|| of the current u."""
+        self._rn2 = self._residual(1.0, False)
+        return math.sqrt(self._rn2) / self.fnorm
 
     def inner(self, m: int) -> None:
-        """m Jacobi sweeps on A e = r from e = 0, then u += e."""
+        """m Jacobi sweeps on the scaled correction equation A e = r / s from e = 0, u += s e.
+
+        s is a power of two at or below the residual's RMS: the correction then stays inside
+        the storage type's exponent range (fp16 would flush a small correction to zero).
+        """
+        ncore = int(np.prod([x - 2 for x in self.shape]))
+        rms = math.sqrt(self._residual(1.0, False) / ncore)
+        sc = math.ldexp(1.0, math.floor(math.log2(rms))) if rms > 0 and math.isfinite(rms) \
+            else 1.0
+        self._residual(1.0 / sc, True)
         self.ea.zero_()
         self.eb.zero_()
         in_b = ctypes.c_int(0)
@@ -128,7 +142,7 @@ class DefectCorrection:
             self.eb.data_ptr(), self.b.data_ptr(), int(m), self._stream(), ctypes.byref(in_b)))
         e = self.eb if in_b.value else self.ea
         _lib.check(self.lib.ph3_dc_correct(self.u.data_ptr(), e.data_ptr(),
-                                           _lib.STORAGE[self.storage], e.numel(),
+                                           _lib.STORAGE[self.storage], sc, e.numel(),
                                            self._stream()))
 
     def solve(self, tol: float = 1e-10, max_outer: int = 60, sweeps: int | list[int] | None = None,

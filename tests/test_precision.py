@@ -114,7 +114,7 @@ def test_gpu_residual_and_dot_kernels_match_numpy():
         out = torch.zeros(1, dtype=torch.float64, device="cuda")
         scr = torch.empty(int(L.ph3_reduction_scratch_len()), dtype=torch.float64, device="cuda")
         nz, ny, nx = (1, *shape) if len(shape) == 2 else shape
-        _lib.check(L.ph3_dc_residual(len(shape), nz, ny, nx, U.data_ptr(), F.data_ptr(), h,
+        _lib.check(L.ph3_dc_residual(len(shape), nz, ny, nx, U.data_ptr(), F.data_ptr(), h, 1.0,
                                      B.data_ptr(), out.data_ptr(), scr.data_ptr(), scr.numel(),
                                      None))
         torch.cuda.synchronize()
