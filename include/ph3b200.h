@@ -171,6 +171,22 @@ int ph3_batch_prepare(const ph3_problem* problems, int n, void* ws, int64_t ws_b
 int ph3_batch_launch(void* ws, int n, void* stream);
 
 /*
+ * ph3_batch_run_static: prepare and launch a batch without any device allocation — for hosts
+ * that cannot call cudaMalloc where they run batches (a serving loop that must not allocate in
+ * steady state, since an allocation can synchronise the device or fail under memory pressure;
+ * a foreign host that hands over field buffers but owns no CUDA allocator). No counterpart in
+ * the reference. The plan and counters live in a fixed 1 MiB device array inside the library
+ * (every GPU that loads the library holds it until exit); problem lists whose plan needs more
+ * (ph3_batch_workspace_bytes > 1 MiB, roughly 8000 problems or 100000 steps) are rejected with
+ * PH3_EINVAL. Every call shares the array: the counters are cleared and the plan rewritten on
+ * each call, and calls that overlap on the GPU race, so the caller must serialise them. The
+ * first call on a device looks up the array's device address (make it before any stream
+ * capture); each call synchronises `stream` after uploading the plan. Results equal
+ * ph3_batch_prepare + ph3_batch_launch bit for bit.
+ */
+int ph3_batch_run_static(const ph3_problem* problems, int n, void* stream);
+
+/*
  * Tuning table (no counterpart in the reference, whose tile constants are module globals that
  * bench/tune.py monkey-patches, cupy_backend.py:50-70). Every family has a few compiled tile
  * configurations; the table holds, per (kernel, dims, storage, k), the configuration index and

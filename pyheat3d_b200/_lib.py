@@ -39,6 +39,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "ph3_batch_workspace_bytes": (_i64, [_p, _i]),
     "ph3_batch_prepare": (_i, [_p, _i, _p, _i64, _p]),
     "ph3_batch_launch": (_i, [_p, _i, _p]),
+    "ph3_batch_run_static": (_i, [_p, _i, _p]),
     "ph3_tune_count": (_i, [_i, _i, _i]),
     "ph3_tune_name": (ctypes.c_char_p, [_i, _i, _i, _i]),
     "ph3_tune_set": (_i, [_i, _i, _i, _i, _i, _i]),

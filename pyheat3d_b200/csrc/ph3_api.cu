@@ -366,6 +366,32 @@ int ph3_batch_launch(void* ws, int n, void* stream) {
                   "batch launch");
 }
 
+int ph3_batch_run_static(const ph3_problem* problems, int n, void* stream) {
+    if (n < 0 || (n > 0 && problems == nullptr))
+        return fail(PH3_EINVAL, "problems must be non-null and n >= 0");
+    for (int i = 0; i < n; ++i) {
+        const ph3_problem& p = problems[i];
+        int rc = check_grid(p.dims, p.dims == 2 ? 1 : p.nz, p.ny, p.nx, p.storage, p.bc);
+        if (rc == PH3_OK) rc = check_ptrs(p.a, p.b, p.src);
+        if (rc != PH3_OK) {
+            char msg[512];
+            snprintf(msg, sizeof(msg), "%s", g_err);
+            return fail(rc, "problem %d: %s", i, msg);
+        }
+        if (p.steps < 0) return fail(PH3_EINVAL, "problem %d: steps must be >= 0", i);
+        if (p.reserved != 0) return fail(PH3_EINVAL, "problem %d: reserved must be 0", i);
+    }
+    long long need = 0;
+    const cudaError_t e =
+        batch_run_static(problems, n, status_ptr(), static_cast<cudaStream_t>(stream), &need);
+    if (e == cudaErrorInvalidValue && need > batch_static_capacity())
+        return fail(PH3_EINVAL,
+                    "batch plan needs %lld bytes; the static workspace holds %lld bytes "
+                    "(use ph3_batch_prepare with a larger workspace)",
+                    need, batch_static_capacity());
+    return finish(e, "batch run (static workspace)");
+}
+
 static thread_local char g_name[64];
 
 static int check_tune_key(int kernel, int dims, int storage, int k) {

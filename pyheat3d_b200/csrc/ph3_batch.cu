@@ -20,6 +20,7 @@
 //   [header][descriptors][order (i32)][tile prefix (i64)][round offsets (i64)]
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -218,6 +219,8 @@ Layout layout_of(int n, int max_steps) {
 }  // namespace
 
 // -------------------------------------------------------------------------------- host API
+cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream);
+
 long long batch_workspace_bytes(const ph3_problem* p, int n) {
     int max_steps = 0;
     for (int i = 0; i < n; ++i) max_steps = std::max(max_steps, p[i].steps);
@@ -273,6 +276,102 @@ cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_by
     e = cudaStreamSynchronize(stream);  // the staging image is freed on return
     if (total_items != nullptr) *total_items = h.total_items;
     return e;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free variant (ph3_batch_run_static). Some hosts cannot allocate device memory at
+// the point where they want to run a batch: a serving loop that must not allocate once it is in
+// steady state (an allocation can synchronise the device or fail under memory pressure), or a
+// foreign host (Go, Java, a plugin) that hands over field buffers but owns no CUDA allocator.
+// For them the plan and counters live in this file-scope device array: 1 MiB on every GPU that
+// loads the library, held until the process exits. Every call shares it, so calls that overlap
+// on the GPU (two streams, two host threads) race and must be serialised by the caller; the
+// counters are cleared on every call, the plan is rewritten on every call.
+// ---------------------------------------------------------------------------------------------
+constexpr long long kStaticWsBytes = 1LL << 20;
+static __device__ __align__(256) unsigned char g_static_ws[kStaticWsBytes];
+
+namespace {
+
+std::mutex g_static_mu;                          // serialises the host-side plan image
+unsigned char g_static_img[kStaticWsBytes];      // host staging of the plan (no heap use)
+
+// Device address of g_static_ws on the current device, looked up once per device.
+unsigned char* static_ws_device(cudaError_t* err) {
+    static unsigned char* ptrs[64] = {nullptr};
+    int dev = 0;
+    *err = cudaGetDevice(&dev);
+    if (*err != cudaSuccess) return nullptr;
+    if (dev < 0 || dev >= 64) {
+        *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    if (ptrs[dev] == nullptr) {
+        void* p = nullptr;
+        *err = cudaGetSymbolAddress(&p, g_static_ws);
+        if (*err != cudaSuccess) return nullptr;
+        ptrs[dev] = static_cast<unsigned char*>(p);
+    }
+    return ptrs[dev];
+}
+
+}  // namespace
+
+long long batch_static_capacity() { return kStaticWsBytes; }
+
+cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t stream,
+                             long long* need_bytes) {
+    int max_steps = 0;
+    for (int i = 0; i < n; ++i) max_steps = std::max(max_steps, p[i].steps);
+    const Layout L = layout_of(n, max_steps);
+    if (need_bytes != nullptr) *need_bytes = L.total;
+    if (L.total > kStaticWsBytes) return cudaErrorInvalidValue;
+    cudaError_t e = cudaSuccess;
+    unsigned char* ws = static_ws_device(&e);
+    if (ws == nullptr) return e;
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    unsigned char* img = g_static_img;
+    std::memset(img, 0, size_t(L.total - L.header));
+    BatchDesc* d = reinterpret_cast<BatchDesc*>(img + L.desc);
+    for (int i = 0; i < n; ++i) {
+        BatchDesc& x = d[i];
+        x.a = p[i].a; x.b = p[i].b; x.src = p[i].src;
+        x.dims = p[i].dims; x.nz = p[i].dims == 2 ? 1 : p[i].nz; x.ny = p[i].ny; x.nx = p[i].nx;
+        x.periodic = p[i].bc == PH3_PERIODIC ? 1 : 0;
+        x.storage = p[i].storage;
+        x.c0 = p[i].c0; x.c1 = p[i].c1;
+        x.steps = p[i].steps;
+        tiles_of(x);
+    }
+    int* order = reinterpret_cast<int*>(img + L.order);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::sort(order, order + n, [&](int a, int b) {
+        return d[a].steps != d[b].steps ? d[a].steps > d[b].steps : a < b;
+    });
+    long long* tilepre = reinterpret_cast<long long*>(img + L.tilepre);
+    tilepre[0] = 0;
+    for (int q = 0; q < n; ++q) tilepre[q + 1] = tilepre[q] + d[order[q]].ntiles;
+    long long* round = reinterpret_cast<long long*>(img + L.round);
+    round[0] = 0;
+    int active = n;
+    for (int s = 0; s < max_steps; ++s) {
+        while (active > 0 && d[order[active - 1]].steps <= s) --active;
+        round[s + 1] = round[s] + tilepre[active];
+    }
+    BatchHeader* h = reinterpret_cast<BatchHeader*>(img);
+    h->n = n;
+    h->max_steps = max_steps;
+    h->total_items = round[max_steps];
+    h->off_desc = L.desc;
+    h->off_order = L.order;
+    h->off_tilepre = L.tilepre;
+    h->off_round = L.round;
+    e = cudaMemcpyAsync(ws + L.header, img, size_t(L.total - L.header), cudaMemcpyHostToDevice,
+                        stream);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(stream);  // the staging image is reused by the next call
+    if (e != cudaSuccess) return e;
+    return batch_launch(ws, n, err, stream);
 }
 
 cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream) {

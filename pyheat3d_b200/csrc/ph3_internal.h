@@ -62,6 +62,9 @@ long long batch_workspace_bytes(const ph3_problem* p, int n);
 cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_bytes,
                           cudaStream_t stream, long long* total_items);
 cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream);
+long long batch_static_capacity();
+cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t stream,
+                             long long* need_bytes);
 
 // Number of streaming multiprocessors of the current device (cached per device).
 int sm_count();
