@@ -60,6 +60,11 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--no-variants", action="store_true", help="skip the per-variant table")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batching measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--no-precision", action="store_true", help="skip the precision measurement")
+    ap.add_argument("--serve-seconds", type=float, default=5.0,
+                    help="length of the Poisson request stream (2000 req/s)")
     ap.add_argument("--variant", default="b200/zmarch",
                     help="kernel of the headline line (b200/zmarch; others for profiling)")
     ap.add_argument("--n", type=int, default=N3,
@@ -373,6 +378,20 @@ def run_b200(a: argparse.Namespace) -> None:
                "sample_1core": "NumPy oracle, 4 updates of the 512^3 field, 1 thread "
                                "(pyheat3d numpy/slicing)"}
 
+    extra = {}
+    if ws == 1:
+        for name, flag, fn in (("precision", a.no_precision, lambda: bench_precision(torch)),
+                               ("batching", a.no_batch, lambda: bench_batching(torch)),
+                               ("serving", a.no_serve,
+                                lambda: bench_serving(torch, a.serve_seconds))):
+            if flag:
+                continue
+            try:
+                extra[name] = fn()
+            except Exception as e:  # reported in the line, the headline stands
+                extra[name] = {"error": f"{type(e).__name__}: {e}"[:300]}
+            torch.cuda.empty_cache()
+
     if rank == 0:
         traffic = profile_traffic("zmarch_tma_512cubed_fp32.md")
         line = {
@@ -399,6 +418,7 @@ def run_b200(a: argparse.Namespace) -> None:
             "clocks": clocks,
             "cpu_baseline": cpu,
             "variants": variants,
+            **extra,
             "finite": final_ok,
         }
         print(json.dumps(line))
@@ -406,6 +426,120 @@ def run_b200(a: argparse.Namespace) -> None:
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------
+# configs 3-5: precision, batching, serving (1-GPU runs; reported beside the headline)
+# ---------------------------------------------------------------------------------------------
+def bench_batching(torch) -> dict:
+    """512 uneven grids (config 4): one persistent launch in a CUDA graph vs per-grid launches."""
+    import ctypes
+
+    from oracle import run_reference
+    from pyheat3d_b200 import _lib
+    from pyheat3d_b200.batch import Batch, synthetic_batch
+
+    probs = synthetic_batch(512, seed=0)
+    batch = Batch(probs)
+    upd = batch.updates
+    g = batch.graph(with_reset=True)
+    g.replay()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(2):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        g.replay()
+        e.record()
+        e.synchronize()
+        times.append(s.elapsed_time(e) * 1e-3)
+    batched = min(times)
+    outs = {i: batch.result_tensor(i).float().cpu().numpy() for i in range(len(probs))}
+    # plain path: one ph3_advance per grid on the same buffers
+    L = _lib.lib()
+    ib = ctypes.c_int(0)
+
+    def plain():
+        st = torch.cuda.current_stream().cuda_stream
+        for i, _ in enumerate(probs):
+            d = batch.descs[i]
+            _lib.check(L.ph3_advance(d.dims, d.nz, d.ny, d.nx, d.storage, d.bc, d.c0, d.c1, 1,
+                                     1, d.a, d.b, d.src, d.steps, st, ctypes.byref(ib)))
+
+    batch.reset()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain()
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    same = all(np.array_equal(outs[i], batch.result_tensor(i).float().cpu().numpy())
+               for i in range(0, len(probs), 37))
+    # FP64-oracle error on the smallest problems of each storage type
+    errs = {}
+    order = sorted(range(len(probs)), key=lambda i: probs[i].cells * probs[i].steps)
+    for st_name in ("float32", "bfloat16"):
+        picked = [i for i in order if probs[i].storage == st_name][:4]
+        worst = 0.0
+        for i in picked:
+            p = probs[i]
+            ref = run_reference(p.u0.astype(np.float64), p.stencil.c0, p.stencil.c1,
+                                p.stencil.bc, p.steps)
+            worst = max(worst, float(np.abs(outs[i] - ref).max() / np.abs(ref).max()))
+        errs[st_name] = worst
+    del batch, g
+    torch.cuda.empty_cache()
+    return {"problems": len(probs), "updates": upd,
+            "batched_s": round(batched, 4), "batched_solves_per_s": round(len(probs) / batched, 2),
+            "batched_glups": round(upd / batched / 1e9, 2),
+            "plain_s": round(plain_s, 4), "plain_solves_per_s": round(len(probs) / plain_s, 2),
+            "plain_glups": round(upd / plain_s / 1e9, 2),
+            "speedup": round(plain_s / batched, 3), "bitwise_equal_to_plain": bool(same),
+            "fp64_oracle_rel_err_smallest4": errs, "graph": True}
+
+
+def bench_serving(torch, seconds: float) -> dict:
+    """Poisson stream, 2000 req/s (config 5): continuous batching vs one solve at a time."""
+    from pyheat3d_b200.serve import GpuExecutor, PlainServer, Server, poisson_stream
+
+    reqs = poisson_stream(2000.0, seconds, seed=0)
+    ex = GpuExecutor()
+    eng = Server(ex, budget_bytes=150e9, quantum=64).run(reqs, duration=seconds, drain=False)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    plain = PlainServer(ex, quantum=64).run(reqs, duration=seconds)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return {"rate_per_s": 2000.0, "stream_s": seconds, "budget_gb": 150.0,
+            "engine": eng.summary(), "plain": plain.summary(),
+            "note": "offered load exceeds one B200 (about 1.7e12 site updates/s of heat work "
+                    "alone); both servers stop at the end of the stream, unfinished requests "
+                    "are the backlog"}
+
+
+def bench_precision(torch, n: int = 256) -> dict:
+    """3D Poisson 256^3 by FP64 defect correction around 16-bit Jacobi (config 3)."""
+    from oracle.precision import discrete_solution, manufactured
+    from pyheat3d_b200.precision import DefectCorrection
+
+    h = 1.0 / (n - 1)
+    u_exact, f = manufactured(n, 3)
+    u_h = discrete_solution(n, 3)
+    out = {}
+    for storage in ("bfloat16", "float16"):
+        dc = DefectCorrection(f, h, storage, "march")
+        res = dc.solve(tol=1e-10, max_outer=40)
+        u = res.host()
+        out[storage] = {
+            "converged": res.converged, "rel_residual": res.history[-1], "outer": res.outer,
+            "sweeps": res.sweeps, "seconds": round(res.seconds, 3),
+            "sweep_glups": round(res.sweeps * (n - 2) ** 3 / res.seconds / 1e9, 2),
+            "err_vs_fp64_oracle": float(np.abs(u - u_h).max() / np.abs(u_h).max()),
+            "err_vs_exact": float(np.abs(u - u_exact).max() / np.abs(u_exact).max()),
+        }
+        del dc, res
+        torch.cuda.empty_cache()
+    return {"grid": [n, n, n], "tol": 1e-10, "fp64_oracle": "exact discrete solution "
+            "(the manufactured f is an eigenfunction of the 7-point Laplacian)", **out}
 
 
 # ---------------------------------------------------------------------------------------------
