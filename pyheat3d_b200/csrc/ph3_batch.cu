@@ -10,7 +10,9 @@
 // waits for items handed out before its own, which are held by running blocks that never wait
 // for later items, so the launch always makes progress.
 //
-// Field reads go through L2 only (__ldcg): other blocks of the same launch write the fields.
+// Tiles are the lean one-column-per-lane marches of ph3_march.cuh (any row alignment, no block
+// barrier inside a tile). Field reads go through L2 only (__ldcg): other blocks of the same
+// launch write the fields.
 // The item list is implicit: a plan in device memory (problem descriptors, the problems sorted
 // by steps, prefix sums of their tile counts and per-round item offsets) lets a block decode an
 // item number with two binary searches.
@@ -52,11 +54,10 @@ struct BatchHeader {
 };
 
 constexpr int kW = 8;          // warps per block
-constexpr int kV = 4;          // values per lane (16-bit storage: 8-byte lane vectors)
-constexpr int kR = 2;          // rows per warp (3D tiles)
-constexpr int kZch = 16;       // planes per 3D tile
-constexpr int kRB2 = 2;        // rows per iteration (2D tiles)
-constexpr int kYch = 64;       // rows per 2D tile
+constexpr int kR = 4;          // rows per warp (3D tiles)
+constexpr int kZch = 32;       // planes per 3D tile
+constexpr int kRB2 = 4;        // rows per iteration (2D tiles)
+constexpr int kYch = 128;      // rows per 2D tile
 constexpr int kThreads = 32 * kW;
 
 __host__ __device__ __forceinline__ long long counter_bytes(int n) {
@@ -73,17 +74,20 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 // Not inlined: each (storage, boundary) tile body keeps its own register allocation instead of
 // the kernel carrying the union of all six.
 template <typename T, bool PER>
-__device__ __noinline__ void run_tile(const BatchDesc& d, int s, int t, float* edge) {
+__device__ __noinline__ void run_tile(const BatchDesc& d, int s, int t) {
     const T* src = static_cast<const T*>((s & 1) ? d.b : d.a);
     T* dst = static_cast<T*>((s & 1) ? d.a : d.b);
+    const int w = threadIdx.x >> 5;
     if (d.dims == 3) {
         const int tx = t % d.ntx, ty = (t / d.ntx) % d.nty, tz = t / (d.ntx * d.nty);
-        march3d_item<T, PER, kV, kR, kW, true>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1, tx,
-                                               ty, tz, kZch, d.vec != 0, edge);
+        const int z0 = tz * kZch;
+        lite3d_item<T, PER, kR, true>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1, tx,
+                                      (ty * kW + w) * kR, z0, min(z0 + kZch, d.nz));
     } else {
         const int tx = t % d.ntx, ty = t / d.ntx;
-        march2d_item<T, PER, kV, kW, kRB2, true>(src, dst, d.src, d.ny, d.nx, d.c0, d.c1,
-                                                 tx * kW, ty, kYch, d.vec != 0);
+        const int y0 = ty * kYch;
+        lite2d_item<T, PER, kRB2, true>(src, dst, d.src, d.ny, d.nx, d.c0, d.c1, tx * kW + w, y0,
+                                        min(y0 + kYch, d.ny));
     }
 }
 
@@ -97,9 +101,8 @@ __device__ __forceinline__ long long upper_bound_i64(const long long* a, int n, 
     return lo;
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 3)
 batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
-    __shared__ __align__(16) float edge[2 * kW * 32 * kV];
     __shared__ int s_p, s_s, s_t;
     __shared__ long long s_item;
     unsigned long long* next = reinterpret_cast<unsigned long long*>(ws);
@@ -148,12 +151,12 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
         const BatchDesc d = desc[s_p];
         const int s = s_s, t = s_t;
         switch (d.storage * 2 + d.periodic) {
-            case 0: run_tile<float, false>(d, s, t, edge); break;
-            case 1: run_tile<float, true>(d, s, t, edge); break;
-            case 2: run_tile<__half, false>(d, s, t, edge); break;
-            case 3: run_tile<__half, true>(d, s, t, edge); break;
-            case 4: run_tile<__nv_bfloat16, false>(d, s, t, edge); break;
-            default: run_tile<__nv_bfloat16, true>(d, s, t, edge); break;
+            case 0: run_tile<float, false>(d, s, t); break;
+            case 1: run_tile<float, true>(d, s, t); break;
+            case 2: run_tile<__half, false>(d, s, t); break;
+            case 3: run_tile<__half, true>(d, s, t); break;
+            case 4: run_tile<__nv_bfloat16, false>(d, s, t); break;
+            default: run_tile<__nv_bfloat16, true>(d, s, t); break;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -182,22 +185,17 @@ int cdiv(long long a, long long b) { return int((a + b - 1) / b); }
 
 // Geometry of one problem's tiles (must match run_tile / the item functions).
 void tiles_of(BatchDesc& d) {
-    const int es = d.storage == kF32 ? 4 : 2;
-    const int EX = 32 * kV;
     if (d.dims == 3) {
-        d.ntx = cdiv(d.nx, EX);
+        d.ntx = cdiv(d.nx, 32);
         d.nty = cdiv(d.ny, kW * kR);
         d.ntz = cdiv(d.nz, kZch);
     } else {
-        d.ntx = cdiv(cdiv(d.nx, EX), kW);
+        d.ntx = cdiv(cdiv(d.nx, 32), kW);
         d.nty = cdiv(d.ny, kYch);
         d.ntz = 1;
     }
     d.ntiles = d.ntx * d.nty * d.ntz;
-    auto al = [&](const void* p, int bytes) {
-        return p == nullptr || reinterpret_cast<uintptr_t>(p) % bytes == 0;
-    };
-    d.vec = (d.nx % kV == 0) && al(d.a, es * kV) && al(d.b, es * kV) && al(d.src, 4 * kV);
+    d.vec = 0;  // the lean tiles take any row alignment
 }
 
 struct Layout {

@@ -304,4 +304,143 @@ __device__ __forceinline__ void march3d_item(const T* __restrict__ u, T* __restr
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// Lean marches for any row alignment: one column per lane, so every row access of a warp is one
+// coalesced 128-byte scalar load or store whatever nx is. Warps are fully independent (no shared
+// memory, no block barrier): a warp owns R rows of a 32-column strip, keeps the z-queue (3D) or
+// a row window (2D) in registers with the next plane / rows already in flight, takes
+// x-neighbours by shuffles (lane 0 / 31 hold the strip's halo column in one register per row)
+// and, in 3D, loads the rows just above and below its own rows directly.
+// ------------------------------------------------------------------------------------------
+template <typename T, bool PER, int R, bool CG>
+__device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restrict__ o,
+                                            const float* __restrict__ b, int nz, int ny, int nx,
+                                            float c0, float c1, int strip, int row0, int zlo,
+                                            int zhi) {
+    const int lane = threadIdx.x & 31;
+    const int x0 = strip * 32, x = x0 + lane;
+    if (x0 >= nx || row0 >= ny) return;  // warp-uniform
+    if constexpr (!PER) { zlo = max(zlo, 1); zhi = min(zhi, nz - 1); }
+    if (zlo >= zhi) return;
+    const int64_t P = int64_t(nx) * ny;
+    const int cx = fix_idx<PER>(x, nx);
+    const int hcol = lane == 0 ? fix_idx<PER>(x0 - 1, nx) : fix_idx<PER>(x0 + 32, nx);
+    const bool hl = lane == 0 || lane == 31;
+    int roff[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) roff[r] = fix_idx<PER>(row0 + r, ny) * nx;
+    const int uoff = fix_idx<PER>(row0 - 1, ny) * nx, doff = fix_idx<PER>(row0 + R, ny) * nx;
+    bool xskip = x >= nx;
+    uint32_t yskip = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (row0 + r >= ny || (!PER && (row0 + r == 0 || row0 + r == ny - 1))) yskip |= 1u << r;
+    if constexpr (!PER) xskip = xskip || x == 0 || x == nx - 1;
+
+    struct Plane {
+        float v[R], h[R];  // own rows; halo column (lanes 0 / 31)
+        float up, dn;      // rows above / below the warp's rows
+    };
+    auto load = [&](int z, Plane& p) {
+        const T* pl = u + int64_t(fix_idx<PER>(z, nz)) * P;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            p.v[r] = ldx1<CG>(pl + roff[r] + cx);
+            p.h[r] = hl ? ldx1<CG>(pl + roff[r] + hcol) : 0.f;
+        }
+        p.up = ldx1<CG>(pl + uoff + cx);
+        p.dn = ldx1<CG>(pl + doff + cx);
+    };
+    float bel[R];
+    {
+        const T* pl = u + int64_t(fix_idx<PER>(zlo - 1, nz)) * P;
+#pragma unroll
+        for (int r = 0; r < R; ++r) bel[r] = ldx1<CG>(pl + roff[r] + cx);
+    }
+    Plane ctr, abv, pre;
+    load(zlo, ctr);
+    load(zlo + 1, abv);
+    for (int z = zlo; z < zhi; ++z) {
+        const bool more = z + 1 < zhi;
+        if (more) load(z + 2, pre);
+        const float* bpl = b != nullptr ? b + int64_t(z) * P : nullptr;
+        T* opl = o + int64_t(z) * P;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float c = ctr.v[r];
+            float xm = __shfl_up_sync(kFull, c, 1);
+            float xp = __shfl_down_sync(kFull, c, 1);
+            if (lane == 0) xm = ctr.h[r];
+            if (lane == 31) xp = ctr.h[r];
+            const float ym = r > 0 ? ctr.v[r - 1] : ctr.up;
+            const float yp = r < R - 1 ? ctr.v[r + 1] : ctr.dn;
+            float v = upd3(c0, c1, c, xm, xp, ym, yp, bel[r], abv.v[r]);
+            if (bpl != nullptr) v = __fadd_rn(v, __ldg(bpl + roff[r] + cx));
+            if (!xskip && !((yskip >> r) & 1u)) opl[roff[r] + x] = from_f<T>(v);
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) bel[r] = ctr.v[r];
+        ctr = abv;
+        if (more) abv = pre;
+    }
+}
+
+template <typename T, bool PER, int RB, bool CG>
+__device__ __forceinline__ void lite2d_item(const T* __restrict__ u, T* __restrict__ o,
+                                            const float* __restrict__ b, int ny, int nx,
+                                            float c0, float c1, int strip, int ylo, int yhi) {
+    const int lane = threadIdx.x & 31;
+    const int x0 = strip * 32, x = x0 + lane;
+    if (x0 >= nx) return;  // warp-uniform
+    if constexpr (!PER) { ylo = max(ylo, 1); yhi = min(yhi, ny - 1); }
+    if (ylo >= yhi) return;
+    const int cx = fix_idx<PER>(x, nx);
+    const int hcol = lane == 0 ? fix_idx<PER>(x0 - 1, nx) : fix_idx<PER>(x0 + 32, nx);
+    const bool hl = lane == 0 || lane == 31;
+    bool xskip = x >= nx;
+    if constexpr (!PER) xskip = xskip || x == 0 || x == nx - 1;
+    // window rows ylo-1 .. ylo+RB and their halo values; the next RB rows in flight
+    float win[RB + 2], wh[RB + 2], pre[RB], ph[RB];
+    auto row = [&](int y) { return u + int64_t(fix_idx<PER>(y, ny)) * nx; };
+#pragma unroll
+    for (int q = 0; q < RB + 2; ++q) {
+        const T* rp = row(ylo - 1 + q);
+        win[q] = ldx1<CG>(rp + cx);
+        wh[q] = hl ? ldx1<CG>(rp + hcol) : 0.f;
+    }
+    for (int y = ylo; y < yhi; y += RB) {
+        const bool more = y + RB < yhi;
+        if (more) {
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+                const T* rp = row(y + RB + 1 + q);
+                pre[q] = ldx1<CG>(rp + cx);
+                ph[q] = hl ? ldx1<CG>(rp + hcol) : 0.f;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < RB; ++q) {
+            const int yy = y + q;
+            if (yy >= yhi) break;
+            const float c = win[q + 1];
+            float xm = __shfl_up_sync(kFull, c, 1);
+            float xp = __shfl_down_sync(kFull, c, 1);
+            if (lane == 0) xm = wh[q + 1];
+            if (lane == 31) xp = wh[q + 1];
+            float v = upd2(c0, c1, c, xm, xp, win[q], win[q + 2]);
+            if (b != nullptr) v = __fadd_rn(v, __ldg(b + int64_t(yy) * nx + cx));
+            if (!xskip) o[int64_t(yy) * nx + x] = from_f<T>(v);
+        }
+        if (more) {
+            win[0] = win[RB]; wh[0] = wh[RB];
+            win[1] = win[RB + 1]; wh[1] = wh[RB + 1];
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+                win[q + 2] = pre[q];
+                wh[q + 2] = ph[q];
+            }
+        }
+    }
+}
+
 }  // namespace ph3

@@ -309,6 +309,25 @@ tb2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict_
     }
 }
 
+template <typename T, bool PER, int R, int W>
+__global__ void __launch_bounds__(32 * W)
+lite3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
+              int ny, int nx, float c0, float c1, int zch) {
+    const int w = threadIdx.x >> 5;
+    const int z0 = blockIdx.z * zch;
+    lite3d_item<T, PER, R, false>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x,
+                                  (blockIdx.y * W + w) * R, z0, min(z0 + zch, nz));
+}
+
+template <typename T, bool PER, int RB, int W>
+__global__ void __launch_bounds__(32 * W)
+lite2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int ny,
+              int nx, float c0, float c1, int ych) {
+    const int y0 = blockIdx.y * ych;
+    lite2d_item<T, PER, RB, false>(u, o, b, ny, nx, c0, c1, blockIdx.x * W + (threadIdx.x >> 5),
+                                   y0, min(y0 + ych, ny));
+}
+
 // ------------------------------------------------------------------------------------------
 // host launchers
 // ------------------------------------------------------------------------------------------
@@ -354,6 +373,30 @@ static cudaError_t march_k1_t(const Launch& L) {
     const T* u = static_cast<const T*>(L.u);
     T* o = static_cast<T*>(L.out);
     const long long target = 8LL * sm_count();
+    // default: lean one-column-per-lane march in 3D (2.1-2.4x the vector march on unaligned
+    // grids on a B200), the vector march in 2D (1.3-1.4x the lean one)
+    const int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : 1);
+    if (cfg == 0) {
+        if (L.dims == 2) {
+            constexpr int W = 4, RB = 4;
+            const int strips = cdiv(L.nx, 32);
+            const int ych = L.chunk > 0 ? L.chunk
+                                        : default_chunk(L.ny, cdiv(strips, W), 8 * RB, 2 * target);
+            dim3 grd(cdiv(strips, W), cdiv(L.ny, ych));
+            if (grd.y > 65535) return cudaErrorInvalidConfiguration;
+            lite2d_kernel<T, PER, RB, W><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.ny, L.nx,
+                                                                      L.c0, L.c1, ych);
+        } else {
+            constexpr int R = 4, W = 4;
+            const long long tiles = 1LL * cdiv(L.nx, 32) * cdiv(L.ny, W * R);
+            const int zch = L.chunk > 0 ? L.chunk : default_chunk(L.nz, tiles, 16, 2 * target);
+            dim3 grd(cdiv(L.nx, 32), cdiv(L.ny, W * R), cdiv(L.nz, zch));
+            if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
+            lite3d_kernel<T, PER, R, W><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.nz, L.ny,
+                                                                     L.nx, L.c0, L.c1, zch);
+        }
+        return cudaGetLastError();
+    }
     if (L.dims == 2) {
         constexpr int V = 16 / sizeof(T), W = 4, RB = sizeof(T) == 4 ? 4 : 2;
         const int strips = cdiv(L.nx, 32 * V);
@@ -447,8 +490,9 @@ cudaError_t launch_tb(const Launch& L) {
 }
 
 int march_configs(int dims, const char** names, int max) {
-    if (names != nullptr && max > 0) names[0] = dims == 2 ? "V16B_W4_RB4" : "V16B_R2_W8";
-    return 1;
+    if (names != nullptr && max > 0) names[0] = dims == 2 ? "lane1_W4_RB4" : "lane1_R4_W4";
+    if (names != nullptr && max > 1) names[1] = dims == 2 ? "V16B_W4_RB4" : "V16B_R2_W8";
+    return 2;
 }
 
 int tb_configs(int dims, int k, const char** names, int max) {
