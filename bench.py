@@ -503,10 +503,11 @@ def bench_serving(torch, seconds: float) -> dict:
 
     reqs = poisson_stream(2000.0, seconds, seed=0)
     ex = GpuExecutor()
-    eng = Server(ex, budget_bytes=150e9, quantum=64).run(reqs, duration=seconds, drain=False)
+    eng = Server(ex, budget_bytes=150e9, max_active=256, quantum=128).run(
+        reqs, duration=seconds, drain=False)
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
-    plain = PlainServer(ex, quantum=64).run(reqs, duration=seconds)
+    plain = PlainServer(ex, quantum=128).run(reqs, duration=seconds)
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     return {"rate_per_s": 2000.0, "stream_s": seconds, "budget_gb": 150.0,
@@ -527,10 +528,11 @@ def bench_precision(torch, n: int = 256) -> dict:
     out = {}
     for storage in ("bfloat16", "float16"):
         dc = DefectCorrection(f, h, storage, "march")
-        res = dc.solve(tol=1e-10, max_outer=40)
+        res = dc.solve(tol=1e-10)
         u = res.host()
         out[storage] = {
             "converged": res.converged, "rel_residual": res.history[-1], "outer": res.outer,
+            "inner_sweeps_per_outer": int(res.sweeps / max(res.outer, 1)),
             "sweeps": res.sweeps, "seconds": round(res.seconds, 3),
             "sweep_glups": round(res.sweeps * (n - 2) ** 3 / res.seconds / 1e9, 2),
             "err_vs_fp64_oracle": float(np.abs(u - u_h).max() / np.abs(u_h).max()),

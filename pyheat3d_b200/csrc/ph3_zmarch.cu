@@ -311,6 +311,222 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
     }
 }
 
+// First form of the consumer (scalar float registers, modulo stage indexing, no register cap):
+// kept as a selectable configuration because it is measured beside the packed form.
+template <typename T, bool PER, int TY, int NWC, int STAGES>
+__global__ void __launch_bounds__(32 * (NWC + 1))
+zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
+                  const __grid_constant__ CUtensorMap tm_row,
+                  const __grid_constant__ CUtensorMap tm_side, T* __restrict__ o,
+                  const float* __restrict__ b, ZmGeom g, float c0, float c1, int* err) {
+    using C = ZmCfg<T, TY, NWC, STAGES>;
+    constexpr int V = C::V, TX = C::TX, HX = C::HX, RW = C::RW;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    volatile int* issued = reinterpret_cast<volatile int*>(empty + STAGES);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NWC);
+        }
+        *issued = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    const int64_t P = int64_t(g.nx) * g.ny;
+
+    if (warp == NWC) {
+        // ----------------------------------------------------------------- producer warp
+        if (lane == 0) {
+            prefetch_tmap(&tm_body);
+            prefetch_tmap(&tm_row);
+            prefetch_tmap(&tm_side);
+            uint32_t it = 0;
+            for (int item = blockIdx.x; item < g.nitems; item += gridDim.x) {
+                const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty;
+                const int ch = item / (g.ntx * g.nty);
+                const int x0 = tx * TX, y0 = ty * TY;
+                const int zlo = g.zbase + ch * g.zch;
+                const int zhi = min(zlo + g.zch, g.zbase + g.nzi);
+                int ytop = y0 - 1, ybot = y0 + TY, xl = x0 - HX, xr = x0 + TX;
+                if constexpr (PER) {
+                    ytop = y0 == 0 ? g.ny - 1 : y0 - 1;
+                    ybot = y0 + TY >= g.ny ? 0 : y0 + TY;
+                    xl = x0 == 0 ? g.nx - HX : x0 - HX;
+                    xr = x0 + TX >= g.nx ? 0 : x0 + TX;
+                }
+                for (int p = zlo - 1; p <= zhi; ++p, ++it) {
+                    const int s = it % STAGES;
+                    const uint32_t n = it / STAGES;
+                    if (n > 0 && !mbar_wait(&empty[s], (n & 1u) ^ 1u, err)) return;
+                    int pz = p;
+                    if constexpr (PER) pz = p < 0 ? p + g.nz : (p >= g.nz ? p - g.nz : p);
+                    unsigned char* st = smem + s * C::STAGE_BYTES;
+                    constexpr int ROW = TX * int(sizeof(T));
+                    mbar_arrive_expect_tx(&full[s], C::TX_BYTES);
+                    tma_load_3d(st, &tm_row, x0, ytop, pz, &full[s]);
+                    tma_load_3d(st + ROW, &tm_body, x0, y0, pz, &full[s]);
+                    tma_load_3d(st + (TY + 1) * ROW, &tm_row, x0, ybot, pz, &full[s]);
+                    tma_load_3d(st + C::BODY_BYTES, &tm_side, xl, y0, pz, &full[s]);
+                    tma_load_3d(st + C::BODY_BYTES + C::SIDE_BYTES, &tm_side, xr, y0, pz,
+                                &full[s]);
+                    *issued = int(it + 1);
+                }
+            }
+        }
+        return;
+    }
+
+    // --------------------------------------------------------------------- consumer warps
+    const int r0 = warp * RW;  // first tile row of this warp
+    uint32_t it = 0;
+    bool ok = true;
+    auto body_row = [&](int s, int row) -> const T* {
+        return reinterpret_cast<const T*>(smem + s * C::STAGE_BYTES) + row * TX;
+    };
+    auto side = [&](int s, int right) -> const T* {
+        return reinterpret_cast<const T*>(smem + s * C::STAGE_BYTES + C::BODY_BYTES +
+                                          right * C::SIDE_BYTES);
+    };
+    auto release = [&](int s) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    };
+    auto lds_vec = [&](const T* p, float (&v)[V]) {
+        union { uint4 w; T e[V]; } un;
+        un.w = *reinterpret_cast<const uint4*>(p);
+#pragma unroll
+        for (int j = 0; j < V; ++j) v[j] = to_f(un.e[j]);
+    };
+
+    for (int item = blockIdx.x; item < g.nitems && ok; item += gridDim.x) {
+        const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty;
+        const int ch = item / (g.ntx * g.nty);
+        const int x0 = tx * TX, y0 = ty * TY;
+        const int zlo = g.zbase + ch * g.zch;
+        const int zhi = min(zlo + g.zch, g.zbase + g.nzi);
+        const int gx = x0 + lane * V;
+        // masks of sites this thread must not write
+        uint32_t skipx = 0, skipy = 0;
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+            if (gx + j >= g.nx || (!PER && (gx + j == 0 || gx + j == g.nx - 1))) skipx |= 1u << j;
+#pragma unroll
+        for (int r = 0; r < RW; ++r) {
+            const int gy = y0 + r0 + r;
+            if (gy >= g.ny || (!PER && (gy == 0 || gy == g.ny - 1))) skipy |= 1u << r;
+        }
+        // periodic wrap inside a partial tile: the site after column nx-1 / row ny-1 is the
+        // halo loaded from column 0 / row 0
+        const bool wrapx = PER && (gx + V == g.nx) && lane != 31;
+        float bel[RW][V], ctr[RW][V], abv[RW][V];
+
+        // plane zlo-1: only the own values are needed
+        {
+            const int s = it % STAGES;
+            if (!mbar_wait(&full[s], (it / STAGES) & 1u, err)) { ok = false; break; }
+#pragma unroll
+            for (int r = 0; r < RW; ++r) lds_vec(body_row(s, r0 + r + 1) + lane * V, bel[r]);
+            release(s);
+            ++it;
+        }
+        int sc = it % STAGES;  // stage of the centre plane
+        if (!mbar_wait(&full[sc], (it / STAGES) & 1u, err)) { ok = false; break; }
+#pragma unroll
+        for (int r = 0; r < RW; ++r) lds_vec(body_row(sc, r0 + r + 1) + lane * V, ctr[r]);
+        ++it;
+
+        for (int z = zlo; z < zhi; ++z) {
+            const int sa = it % STAGES;
+            if (!mbar_wait(&full[sa], (it / STAGES) & 1u, err)) { ok = false; break; }
+#pragma unroll
+            for (int r = 0; r < RW; ++r) lds_vec(body_row(sa, r0 + r + 1) + lane * V, abv[r]);
+            // y-neighbours of the first and last rows come from the staged centre plane
+            // periodic partial tile: the row after ny-1 is the halo row loaded from row 0
+            int wrap_r = -1;
+            if (PER && y0 + TY > g.ny) {
+                const int rr = g.ny - 1 - (y0 + r0);
+                if (rr >= 0 && rr < RW) wrap_r = rr;
+            }
+            float up[V], dn[V], wdn[V];
+            lds_vec(body_row(sc, r0) + lane * V, up);
+            lds_vec(body_row(sc, wrap_r == RW - 1 ? TY + 1 : r0 + RW + 1) + lane * V, dn);
+            if (wrap_r >= 0 && wrap_r < RW - 1) lds_vec(body_row(sc, TY + 1) + lane * V, wdn);
+            const T* sl = side(sc, 0);
+            const T* sr = side(sc, 1);
+#pragma unroll
+            for (int r = 0; r < RW; ++r) {
+                const int gy = y0 + r0 + r;
+                const float left = __shfl_up_sync(kFullMask, ctr[r][V - 1], 1);
+                const float right = __shfl_down_sync(kFullMask, ctr[r][0], 1);
+                float hl = 0.f, hr = 0.f;
+                if (lane == 0) hl = to_f(sl[(r0 + r) * HX + HX - 1]);
+                if (lane == 31 || wrapx) hr = to_f(sr[(r0 + r) * HX]);
+                float bv[V];
+                if (b != nullptr) {
+                    const float* bp = b + int64_t(z) * P + int64_t(min(gy, g.ny - 1)) * g.nx +
+                                      min(gx, g.nx - V);
+#pragma unroll
+                    for (int q = 0; q < V / 4; ++q) {
+                        const float4 t = __ldg(reinterpret_cast<const float4*>(bp) + q);
+                        bv[4 * q] = t.x; bv[4 * q + 1] = t.y; bv[4 * q + 2] = t.z; bv[4 * q + 3] = t.w;
+                    }
+                }
+                float out[V];
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    const float xm = j > 0 ? ctr[r][j - 1] : (lane == 0 ? hl : left);
+                    const float xp = j < V - 1 ? ctr[r][j + 1]
+                                               : ((lane == 31 || wrapx) ? hr : right);
+                    const float ym = r > 0 ? ctr[r - 1][j] : up[j];
+                    float yp = dn[j];
+                    if (r < RW - 1) yp = r == wrap_r ? wdn[j] : ctr[r + 1][j];
+                    float v = upd3(c0, c1, ctr[r][j], xm, xp, ym, yp, bel[r][j], abv[r][j]);
+                    if (b != nullptr) v = __fadd_rn(v, bv[j]);
+                    out[j] = v;
+                }
+                if (!((skipy >> r) & 1u)) {
+                    T* dst = o + int64_t(z) * P + int64_t(gy) * g.nx + gx;
+                    if (skipx == 0) {
+                        st_vec<T, V>(dst, out);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < V; ++j)
+                            if (!((skipx >> j) & 1u)) dst[j] = from_f<T>(out[j]);
+                    }
+                }
+            }
+            release(sc);
+#pragma unroll
+            for (int r = 0; r < RW; ++r)
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    bel[r][j] = ctr[r][j];
+                    ctr[r][j] = abv[r][j];
+                }
+            sc = sa;
+            ++it;
+        }
+        if (!ok) break;
+        release(sc);  // plane zhi
+    }
+
+    if (!ok) {
+        // a wait expired: drain the loads this block issued so no copy lands after exit
+        if (warp == 0 && lane == 0) {
+            const int n_issued = *issued;
+            for (int k = int(it); k < n_issued; ++k) {
+                const int s = k % STAGES;
+                if (!mbar_wait(&full[s], (uint32_t(k) / STAGES) & 1u, err)) break;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
@@ -349,10 +565,11 @@ bool make_map(CUtensorMap* m, const void* base, int nz, int ny, int nx, int bx, 
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED = true>
+template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED = true, bool V1 = false>
 cudaError_t zmarch_t(const Launch& L) {
     using C = ZmCfg<T, TY, NWC, STAGES>;
-    auto kern = zmarch_tma_kernel<T, PER, TY, NWC, STAGES, PACKED>;
+    auto kern = V1 ? zmarch_v1_kernel<T, PER, TY, NWC, STAGES>
+                   : zmarch_tma_kernel<T, PER, TY, NWC, STAGES, PACKED>;
     static int blocks_per_sm[64] = {0};  // per device
     int dev = 0;
     cudaGetDevice(&dev);
@@ -388,10 +605,11 @@ cudaError_t zmarch_t(const Launch& L) {
         // one-wave z-slab schedule reads 2.5% less but leaves blocks idle and is slower)
         const long long plane_bytes = 1LL * L.nx * L.ny * sizeof(T);
         const long long cap = std::max(8LL, (64LL << 20) / std::max(1LL, 2 * plane_bytes));
-        zch = int(std::min<long long>(cap, 32));
+        // small grids: shorter chunks so that there are about three items per resident block
+        const long long fill = (1LL * g.nzi * tiles + 3 * resident - 1) / (3 * resident);
+        zch = int(std::max(8LL, std::min({cap, 32LL, fill})));
         zch = std::max(1, std::min(zch, g.nzi));
     }
-    (void)resident;
     g.zch = zch;
     g.nchunks = (g.nzi + zch - 1) / zch;
     const long long nitems = tiles * g.nchunks;
@@ -414,8 +632,9 @@ bool zmarch_tma_supported(const Launch& L) {
 
 // Compiled z-march configurations: rows per tile (TY), consumer warps (NWC), ring stages.
 static const char* kZmNames[] = {"TY16_W8_S6", "TY8_W8_S8", "TY32_W8_S4", "TY16_W16_S6",
-                                 "TY8_W4_S8", "TY16_W8_S6_scalar", "TY16_W16_S6_scalar"};
-constexpr int kZmCount = 7;
+                                 "TY8_W4_S8", "TY16_W8_S6_scalar", "TY16_W16_S6_scalar",
+                                 "TY16_W8_S6_v1", "TY16_W16_S6_v1"};
+constexpr int kZmCount = 9;
 
 int zmarch_configs(const char** names, int max) {
     for (int i = 0; i < kZmCount && names != nullptr && i < max; ++i) names[i] = kZmNames[i];
@@ -433,7 +652,9 @@ static cudaError_t zmarch_cfg(const Launch& L) {
         case 3: return zmarch_t<T, PER, 16, 16, 6>(L);
         case 4: return zmarch_t<T, PER, 8, 4, 8>(L);
         case 5: return zmarch_t<T, PER, 16, 8, 6, false>(L);
-        default: return zmarch_t<T, PER, 16, 16, 6, false>(L);
+        case 6: return zmarch_t<T, PER, 16, 16, 6, false>(L);
+        case 7: return zmarch_t<T, PER, 16, 8, 6, true, true>(L);
+        default: return zmarch_t<T, PER, 16, 16, 6, true, true>(L);
     }
 }
 

@@ -13,8 +13,9 @@ The reference solves the Poisson problem with plain Jacobi and the source b = -h
 * u <- u + s e, and the loop stops when ||r||_2 / ||f||_2 <= tol.
 
 ``m`` is chosen from the Jacobi spectral radius rho = cos(pi h) so that one inner solve damps
-the smoothest error mode by the storage type's resolution (``REDUCTION``): reducing further
-gains nothing because e itself is only stored to that precision.
+the smoothest error mode by the storage type's resolution (``REDUCTION``), but never more than
+``MAX_INNER`` sweeps: past that many sweeps from e = 0, one sweep's change of the smooth part of
+e is below half an ulp of the storage type and rounds away.
 """
 
 from __future__ import annotations
@@ -31,6 +32,12 @@ from . import _lib
 #: per-outer-iteration damping target of the inner solve, by storage type
 REDUCTION = {"bfloat16": 2.0**-6, "float16": 2.0**-9, "float32": 2.0**-18}
 
+#: inner sweeps per outer iteration at most, by storage type. Starting from e = 0, sweep k
+#: changes the smooth part of the correction by about e / k; once that falls below half a unit
+#: in the last place of the storage type (k ~ 2^(significand bits)) every further update rounds
+#: away and the inner solve stalls (bf16 stalls after ~256 sweeps on any large grid).
+MAX_INNER = {"bfloat16": 128, "float16": 1024, "float32": 1 << 20}
+
 
 def _torch():
     import torch
@@ -39,10 +46,17 @@ def _torch():
 
 
 def inner_sweeps(n: int, storage: str, k: int = 1) -> int:
-    """Jacobi sweeps that damp the smoothest mode by REDUCTION[storage] (multiple of k)."""
+    """Sweeps per inner solve: enough to damp the smoothest mode by REDUCTION[storage], at most
+    MAX_INNER[storage] (a multiple of k)."""
     rho = math.cos(math.pi / (n - 1))
     m = int(math.ceil(math.log(REDUCTION[storage]) / math.log(rho)))
+    m = min(m, MAX_INNER[storage])
     return max(k, int(math.ceil(m / k)) * k)
+
+
+def jacobi_sweeps(n: int, tol: float) -> int:
+    """Sweeps plain Jacobi needs to damp the smoothest mode by tol (validation.py:89-93)."""
+    return int(math.ceil(math.log(tol) / math.log(math.cos(math.pi / (n - 1)))))
 
 
 @dataclass
@@ -122,14 +136,17 @@ class DefectCorrection:
         self._rn2 = self._residual(1.0, False)
         return math.sqrt(self._rn2) / self.fnorm
 
-    def inner(self, m: int) -> None:
+    def inner(self, m: int, rn2: float | None = None) -> None:
         """m Jacobi sweeps on the scaled correction equation A e = r / s from e = 0, u += s e.
 
         s is a power of two at or below the residual's RMS: the correction then stays inside
         the storage type's exponent range (fp16 would flush a small correction to zero).
+        ``rn2``: sum(r^2) of the current u if already known (saves one residual pass).
         """
         ncore = int(np.prod([x - 2 for x in self.shape]))
-        rms = math.sqrt(self._residual(1.0, False) / ncore)
+        if rn2 is None:
+            rn2 = self._residual(1.0, False)
+        rms = math.sqrt(rn2 / ncore)
         sc = math.ldexp(1.0, math.floor(math.log2(rms))) if rms > 0 and math.isfinite(rms) \
             else 1.0
         self._residual(1.0 / sc, True)
@@ -145,32 +162,35 @@ class DefectCorrection:
                                            _lib.STORAGE[self.storage], sc, e.numel(),
                                            self._stream()))
 
-    def solve(self, tol: float = 1e-10, max_outer: int = 60, sweeps: int | list[int] | None = None,
-              check_every: int = 1) -> DCResult:
-        """Outer iterations until the relative residual is <= tol (or max_outer).
+    def solve(self, tol: float = 1e-10, max_outer: int | None = None,
+              sweeps: int | list[int] | None = None, max_sweeps: int | None = None) -> DCResult:
+        """Outer iterations until the relative residual is <= tol.
 
         ``sweeps``: inner sweeps per outer iteration (int), an explicit schedule (list; the loop
         then runs exactly len(schedule) outer iterations), or None for :func:`inner_sweeps`.
+        The loop also stops after ``max_outer`` outer iterations or ``max_sweeps`` inner sweeps
+        (default: three times what plain Jacobi needs for ``tol``).
         """
         torch = _torch()
         n = min(self.shape)
         schedule = sweeps if isinstance(sweeps, list) else None
         m = sweeps if isinstance(sweeps, int) else inner_sweeps(n, self.storage, self.k)
+        if max_sweeps is None:
+            max_sweeps = 3 * jacobi_sweeps(n, tol)
         torch.cuda.synchronize(self.device)
         t0 = time.perf_counter()
         hist = [self.residual()]
         total = 0
         outer = 0
-        limit = len(schedule) if schedule is not None else max_outer
+        limit = len(schedule) if schedule is not None else (max_outer or 1 << 30)
         while outer < limit:
-            if schedule is None and hist[-1] <= tol:
+            if schedule is None and (hist[-1] <= tol or total >= max_sweeps):
                 break
             mm = schedule[outer] if schedule is not None else m
-            self.inner(mm)
+            self.inner(mm, self._rn2)
             total += mm
             outer += 1
-            if outer % check_every == 0 or outer == limit:
-                hist.append(self.residual())
+            hist.append(self.residual())
         torch.cuda.synchronize(self.device)
         secs = time.perf_counter() - t0
         return DCResult(self.u, hist, outer, total, secs, self.storage,

@@ -217,6 +217,23 @@ class GpuExecutor:
         s.last_change = diff / nrm if nrm > 0 else 0.0
         return s.last_change <= s.req.tol
 
+    def converged_many(self, slots: list[_Slot]) -> list[bool]:
+        """:meth:`converged` for several slots with a single device synchronisation."""
+        torch = self.torch
+        if not slots:
+            return []
+        pairs = []
+        for s in slots:
+            cur, prev = (s.b, s.a) if s.in_b else (s.a, s.b)
+            cf = cur.float()
+            pairs.append(torch.stack([cf.norm(), (cf - prev.float()).norm()]))
+        vals = torch.stack(pairs).cpu().tolist()
+        out = []
+        for s, (nrm, diff) in zip(slots, vals):
+            s.last_change = diff / nrm if nrm > 0 else 0.0
+            out.append(s.done > 0 and s.last_change <= s.req.tol)
+        return out
+
     def fetch(self, s: _Slot) -> np.ndarray:
         return ((s.b if s.in_b else s.a).float()).cpu().numpy()
 
@@ -352,12 +369,16 @@ class Server:
                 updates += slot.req.cells * c
             still = []
             tnow = None
+            jac = [s for s, _ in active if s.req.kind == "jacobi"]
+            many = getattr(self.ex, "converged_many", None)
+            conv_of = dict(zip(map(id, jac), many(jac) if many else
+                               [self.ex.converged(s) for s in jac]))
             for slot, adm in active:
                 req = slot.req
                 if req.kind == "heat":
                     fin, conv = slot.done >= req.steps, True
                 else:
-                    conv = self.ex.converged(slot)
+                    conv = conv_of[id(slot)]
                     fin = conv or slot.done >= req.max_sweeps
                 if fin:
                     res = self.ex.fetch(slot) if self.keep else None
