@@ -644,7 +644,9 @@ int zmarch_configs(const char** names, int max) {
 template <typename T, bool PER>
 static cudaError_t zmarch_cfg(const Launch& L) {
     int cfg = L.cfg;
-    if (cfg < 0 || cfg >= kZmCount) cfg = 3;  // 16 rows x 16 warps: fastest at 512^3
+    // defaults measured on a B200 at 512^3 (1000-step solves, median of 3): fp32 the scalar
+    // consumer with 16 rows x 16 warps (720 GLUPS vs 686 packed), 16-bit the packed 16 x 16
+    if (cfg < 0 || cfg >= kZmCount) cfg = sizeof(T) == 4 ? 8 : 3;
     switch (cfg) {
         case 0: return zmarch_t<T, PER, 16, 8, 6>(L);
         case 1: return zmarch_t<T, PER, 8, 8, 8>(L);
