@@ -393,7 +393,7 @@ def run_b200(a: argparse.Namespace) -> None:
             torch.cuda.empty_cache()
 
     if rank == 0:
-        traffic = profile_traffic("zmarch_tma_512cubed_fp32.md")
+        traffic = profile_traffic("zmarch_tma_512cubed_fp32.md" if a.variant == "b200/zmarch" else "")
         line = {
             "metric": "GLUPS (3D 512^3 fp32 periodic FTCS, single-step TMA z-march)",
             "value": round(value, 2), "kernel": a.variant, "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
