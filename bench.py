@@ -149,7 +149,7 @@ class Clocks:
 def profile_traffic(name: str) -> float | None:
     """DRAM bytes per launch from a committed ncu summary (``dram_bytes_per_launch: N`` line)."""
     p = ROOT / "profiles" / name
-    if not p.exists():
+    if not name or not p.is_file():
         return None
     for line in p.read_text().splitlines():
         if line.strip().startswith("dram_bytes_per_launch:"):
