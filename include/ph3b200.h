@@ -54,6 +54,7 @@ extern "C" {
 #define PH3_KERNEL_MARCH 1  /* plain-load single-step march (2D y-march, 3D unaligned) */
 #define PH3_KERNEL_TB 2     /* temporal blocking, k in {2, 3, 4, 8} */
 #define PH3_KERNEL_NAIVE 3  /* one site per thread (no configurations) */
+#define PH3_KERNEL_BATCH 4  /* batch tiles; one entry, keyed dims 3, PH3_FLOAT32, k 1 */
 
 /* Library version (major*10000 + minor*100 + patch). */
 int ph3_version(void);

@@ -47,7 +47,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
 }
 
 #: tuning-table kernel families (include/ph3b200.h PH3_KERNEL_*)
-KERNEL = {"zmarch": 0, "march": 1, "tb": 2, "naive": 3}
+KERNEL = {"zmarch": 0, "march": 1, "tb": 2, "naive": 3, "batch": 4}
 
 _lock = threading.Lock()
 _lib: ctypes.CDLL | None = None

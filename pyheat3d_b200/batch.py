@@ -97,6 +97,9 @@ class Batch:
             d.steps = int(p.steps)
             d.reserved = 0
         self.n = n
+        from .tune import configure_batch
+
+        configure_batch(self.lib)  # tile configuration from the tuning table, if one is active
         descs = ctypes.addressof(self.descs)
         nbytes = int(self.lib.ph3_batch_workspace_bytes(descs, n))
         if nbytes < 0:

@@ -92,6 +92,7 @@ int family_count(int family, int dims, int k, const char** names, int max) {
         case kFamZmarch: return dims == 3 && k == 1 ? zmarch_configs(names, max) : 0;
         case kFamMarch: return k == 1 ? march_configs(dims, names, max) : 0;
         case kFamTb: return tb_configs(dims, k, names, max);
+        case kFamBatch: return k == 1 ? batch_configs(names, max) : 0;
         default: return 0;
     }
 }
@@ -355,8 +356,10 @@ int ph3_batch_prepare(const ph3_problem* problems, int n, void* ws, int64_t ws_b
     const long long need = batch_workspace_bytes(problems, n);
     if (ws_bytes < need)
         return fail(PH3_EINVAL, "workspace needs %lld bytes, got %lld", need, (long long)ws_bytes);
+    tune_init();  // the batch family's entry (keyed dims 3, fp32, k 1) picks the tile config
+    const int cfg = g_tune_cfg[kFamBatch][1][PH3_FLOAT32][1].load();
     return finish(batch_prepare(problems, n, ws, ws_bytes, static_cast<cudaStream_t>(stream),
-                                nullptr),
+                                nullptr, cfg),
                   "batch prepare");
 }
 
@@ -382,8 +385,10 @@ int ph3_batch_run_static(const ph3_problem* problems, int n, void* stream) {
         if (p.reserved != 0) return fail(PH3_EINVAL, "problem %d: reserved must be 0", i);
     }
     long long need = 0;
-    const cudaError_t e =
-        batch_run_static(problems, n, status_ptr(), static_cast<cudaStream_t>(stream), &need);
+    tune_init();
+    const int cfg = g_tune_cfg[kFamBatch][1][PH3_FLOAT32][1].load();
+    const cudaError_t e = batch_run_static(problems, n, status_ptr(),
+                                           static_cast<cudaStream_t>(stream), &need, cfg);
     if (e == cudaErrorInvalidValue && need > batch_static_capacity())
         return fail(PH3_EINVAL,
                     "batch plan needs %lld bytes; the static workspace holds %lld bytes "

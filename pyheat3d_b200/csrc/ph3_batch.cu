@@ -49,15 +49,31 @@ struct BatchDesc {
 struct BatchHeader {
     int n;
     int max_steps;
+    int cfg;  // tile configuration the descriptors' tile counts were computed for
+    int pad;
     long long total_items;
     long long off_desc, off_order, off_tilepre, off_round;
 };
 
-constexpr int kW = 8;          // warps per block
-constexpr int kR = 4;          // rows per warp (3D tiles)
-constexpr int kZch = 32;       // planes per 3D tile
-constexpr int kRB2 = 4;        // rows per iteration (2D tiles)
-constexpr int kYch = 128;      // rows per 2D tile
+constexpr int kW = 8;  // warps per block
+
+// Compiled tile configurations (the tuning table's batch family): rows per warp and planes per
+// 3D tile, rows per iteration and rows per 2D tile. The plan records which one it was built for.
+template <int CFG> struct BCfg;
+template <> struct BCfg<0> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128; };
+template <> struct BCfg<1> { static constexpr int R = 2, ZCH = 16, RB2 = 4, YCH = 64; };
+template <> struct BCfg<2> { static constexpr int R = 8, ZCH = 64, RB2 = 8, YCH = 256; };
+constexpr int kBatchCfgs = 3;
+const char* kBatchNames[kBatchCfgs] = {"R4_Z32_Y128", "R2_Z16_Y64", "R8_Z64_Y256"};
+
+struct Geo { int R, ZCH, YCH; };
+Geo geo_of(int cfg) {
+    switch (cfg) {
+        case 1: return {BCfg<1>::R, BCfg<1>::ZCH, BCfg<1>::YCH};
+        case 2: return {BCfg<2>::R, BCfg<2>::ZCH, BCfg<2>::YCH};
+        default: return {BCfg<0>::R, BCfg<0>::ZCH, BCfg<0>::YCH};
+    }
+}
 constexpr int kThreads = 32 * kW;
 
 __host__ __device__ __forceinline__ long long counter_bytes(int n) {
@@ -71,23 +87,36 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
     return v;
 }
 
-// Not inlined: each (storage, boundary) tile body keeps its own register allocation instead of
-// the kernel carrying the union of all six.
-template <typename T, bool PER>
+// Not inlined: each (storage, boundary, configuration) tile body keeps its own register
+// allocation instead of the kernel carrying the union of all of them.
+template <typename T, bool PER, int CFG>
 __device__ __noinline__ void run_tile(const BatchDesc& d, int s, int t) {
+    using C = BCfg<CFG>;
     const T* src = static_cast<const T*>((s & 1) ? d.b : d.a);
     T* dst = static_cast<T*>((s & 1) ? d.a : d.b);
     const int w = threadIdx.x >> 5;
     if (d.dims == 3) {
         const int tx = t % d.ntx, ty = (t / d.ntx) % d.nty, tz = t / (d.ntx * d.nty);
-        const int z0 = tz * kZch;
-        lite3d_item<T, PER, kR, true>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1, tx,
-                                      (ty * kW + w) * kR, z0, min(z0 + kZch, d.nz));
+        const int z0 = tz * C::ZCH;
+        lite3d_item<T, PER, C::R, true>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1, tx,
+                                        (ty * kW + w) * C::R, z0, min(z0 + C::ZCH, d.nz));
     } else {
         const int tx = t % d.ntx, ty = t / d.ntx;
-        const int y0 = ty * kYch;
-        lite2d_item<T, PER, kRB2, true>(src, dst, d.src, d.ny, d.nx, d.c0, d.c1, tx * kW + w, y0,
-                                        min(y0 + kYch, d.ny));
+        const int y0 = ty * C::YCH;
+        lite2d_item<T, PER, C::RB2, true>(src, dst, d.src, d.ny, d.nx, d.c0, d.c1, tx * kW + w,
+                                          y0, min(y0 + C::YCH, d.ny));
+    }
+}
+
+template <int CFG>
+__device__ __forceinline__ void run_any(const BatchDesc& d, int s, int t) {
+    switch (d.storage * 2 + d.periodic) {
+        case 0: run_tile<float, false, CFG>(d, s, t); break;
+        case 1: run_tile<float, true, CFG>(d, s, t); break;
+        case 2: run_tile<__half, false, CFG>(d, s, t); break;
+        case 3: run_tile<__half, true, CFG>(d, s, t); break;
+        case 4: run_tile<__nv_bfloat16, false, CFG>(d, s, t); break;
+        default: run_tile<__nv_bfloat16, true, CFG>(d, s, t); break;
     }
 }
 
@@ -116,6 +145,7 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
     const long long* round_off = reinterpret_cast<const long long*>(base + hd->off_round);
     const long long total = hd->total_items;
     const int max_steps = hd->max_steps;
+    const int cfg = hd->cfg;
 
     for (;;) {
         if (threadIdx.x == 0) {
@@ -150,13 +180,10 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
         if (s_item < 0) break;
         const BatchDesc d = desc[s_p];
         const int s = s_s, t = s_t;
-        switch (d.storage * 2 + d.periodic) {
-            case 0: run_tile<float, false>(d, s, t); break;
-            case 1: run_tile<float, true>(d, s, t); break;
-            case 2: run_tile<__half, false>(d, s, t); break;
-            case 3: run_tile<__half, true>(d, s, t); break;
-            case 4: run_tile<__nv_bfloat16, false>(d, s, t); break;
-            default: run_tile<__nv_bfloat16, true>(d, s, t); break;
+        switch (cfg) {
+            case 1: run_any<1>(d, s, t); break;
+            case 2: run_any<2>(d, s, t); break;
+            default: run_any<0>(d, s, t); break;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -184,14 +211,15 @@ int blocks_per_sm_cached() {
 int cdiv(long long a, long long b) { return int((a + b - 1) / b); }
 
 // Geometry of one problem's tiles (must match run_tile / the item functions).
-void tiles_of(BatchDesc& d) {
+void tiles_of(BatchDesc& d, int cfg) {
+    const Geo g = geo_of(cfg);
     if (d.dims == 3) {
         d.ntx = cdiv(d.nx, 32);
-        d.nty = cdiv(d.ny, kW * kR);
-        d.ntz = cdiv(d.nz, kZch);
+        d.nty = cdiv(d.ny, kW * g.R);
+        d.ntz = cdiv(d.nz, g.ZCH);
     } else {
         d.ntx = cdiv(cdiv(d.nx, 32), kW);
-        d.nty = cdiv(d.ny, kYch);
+        d.nty = cdiv(d.ny, g.YCH);
         d.ntz = 1;
     }
     d.ntiles = d.ntx * d.nty * d.ntz;
@@ -226,7 +254,8 @@ long long batch_workspace_bytes(const ph3_problem* p, int n) {
 }
 
 cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_bytes,
-                          cudaStream_t stream, long long* total_items) {
+                          cudaStream_t stream, long long* total_items, int cfg) {
+    if (cfg < 0 || cfg >= kBatchCfgs) cfg = 0;
     std::vector<BatchDesc> d(n);
     int max_steps = 0;
     for (int i = 0; i < n; ++i) {
@@ -237,7 +266,7 @@ cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_by
         x.storage = p[i].storage;
         x.c0 = p[i].c0; x.c1 = p[i].c1;
         x.steps = p[i].steps;
-        tiles_of(x);
+        tiles_of(x, cfg);
         max_steps = std::max(max_steps, x.steps);
     }
     const Layout L = layout_of(n, max_steps);
@@ -257,6 +286,8 @@ cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_by
     BatchHeader h;
     h.n = n;
     h.max_steps = max_steps;
+    h.cfg = cfg;
+    h.pad = 0;
     h.total_items = round[max_steps];
     h.off_desc = L.desc;
     h.off_order = L.order;
@@ -317,8 +348,14 @@ unsigned char* static_ws_device(cudaError_t* err) {
 
 long long batch_static_capacity() { return kStaticWsBytes; }
 
+int batch_configs(const char** names, int max) {
+    for (int i = 0; i < kBatchCfgs && names != nullptr && i < max; ++i) names[i] = kBatchNames[i];
+    return kBatchCfgs;
+}
+
 cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t stream,
-                             long long* need_bytes) {
+                             long long* need_bytes, int cfg) {
+    if (cfg < 0 || cfg >= kBatchCfgs) cfg = 0;
     int max_steps = 0;
     for (int i = 0; i < n; ++i) max_steps = std::max(max_steps, p[i].steps);
     const Layout L = layout_of(n, max_steps);
@@ -339,7 +376,7 @@ cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t
         x.storage = p[i].storage;
         x.c0 = p[i].c0; x.c1 = p[i].c1;
         x.steps = p[i].steps;
-        tiles_of(x);
+        tiles_of(x, cfg);
     }
     int* order = reinterpret_cast<int*>(img + L.order);
     for (int i = 0; i < n; ++i) order[i] = i;
@@ -359,6 +396,7 @@ cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t
     BatchHeader* h = reinterpret_cast<BatchHeader*>(img);
     h->n = n;
     h->max_steps = max_steps;
+    h->cfg = cfg;
     h->total_items = round[max_steps];
     h->off_desc = L.desc;
     h->off_order = L.order;

@@ -38,7 +38,9 @@ bool tbbulk_supported(const Launch& L);
 int tbbulk_configs(int k, const char** names, int max);
 
 // Kernel families with selectable compiled configurations (the tuning table's first index).
-enum Family : int { kFamZmarch = 0, kFamMarch = 1, kFamTb = 2, kFamNaive = 3, kNumFamilies = 4 };
+enum Family : int {
+    kFamZmarch = 0, kFamMarch = 1, kFamTb = 2, kFamNaive = 3, kFamBatch = 4, kNumFamilies = 5
+};
 
 // Names of the compiled configurations of a family for (dims, k); returns how many there are.
 // names may be null. Implemented by the translation unit that owns the family.
@@ -60,11 +62,12 @@ cudaError_t launch_dc_correct(double* u, const void* e, int storage, double scal
 // Batched persistent launch (ph3_batch.cu).
 long long batch_workspace_bytes(const ph3_problem* p, int n);
 cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_bytes,
-                          cudaStream_t stream, long long* total_items);
+                          cudaStream_t stream, long long* total_items, int cfg);
+int batch_configs(const char** names, int max);
 cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream);
 long long batch_static_capacity();
 cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t stream,
-                             long long* need_bytes);
+                             long long* need_bytes, int cfg);
 
 // Number of streaming multiprocessors of the current device (cached per device).
 int sm_count();

@@ -53,6 +53,10 @@ def _build(variant_cls=Variant) -> dict[str, Variant]:
                                  rung=5 if st == "float32" else 6,
                                  description=f"B200 CUDA temporal blocking, {K} steps per DRAM "
                                              f"pass, {st} storage"))
+    v.append(variant_cls(BACKEND, "auto", _factory("auto", "float32", 1), storage="float32",
+                         source=True, rung=7,
+                         description="B200 CUDA, kernel family and temporal-block depth chosen "
+                                     "per grid size by the autotuner's table"))
     return {x.key: x for x in v}
 
 

@@ -15,6 +15,7 @@ import numpy as np
 
 from . import _lib
 from .contract import Stepper
+from .tune import configure
 
 _TORCH_DTYPE_NAMES = {"float32": "float32", "float16": "float16", "bfloat16": "bfloat16"}
 
@@ -38,6 +39,12 @@ class B200Stepper(Stepper):
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device")
         self._lib = _lib.lib()  # fails loudly when the extension is missing
+        if self.kind == "auto":  # kernel family and temporal-block depth from the tuning table
+            from .tune import active_table
+
+            t = active_table()
+            best = t.best_for(self.dims, self.storage, self.ncells) if t is not None else None
+            self.kind, self.K = (best["variant"], int(best["k"])) if best else ("march", 1)
         if self.kind == "march" and self.dims not in (2, 3):  # pragma: no cover
             raise ValueError("march needs a 2D or 3D grid")
         self.steps_per_pass = self.K if self.kind == "tb" else 1
@@ -69,6 +76,7 @@ class B200Stepper(Stepper):
         torch = _torch()
         stream = torch.cuda.current_stream(self.device).cuda_stream
         src = self.src.data_ptr() if self.src is not None else None
+        configure(self.dims, self.storage, self._k, self.ncells, self._lib)
         _lib.check(self._lib.ph3_advance(
             self.dims, self._nz, self._ny, self._nx, _lib.STORAGE[self.storage],
             _lib.BC[self.bc], self._c0, self._c1, self._variant, self._k,
@@ -123,8 +131,11 @@ class B200Stepper(Stepper):
 
 
 def make(kind: str, storage: str = "float32", K: int = 1) -> type[B200Stepper]:
-    """A ``B200Stepper`` subclass for a kernel family, storage type and K (cupy_backend.py:207)."""
-    if kind not in _lib.VARIANT:
+    """A ``B200Stepper`` subclass for a kernel family, storage type and K (cupy_backend.py:207).
+
+    ``kind="auto"`` picks family and K per grid from the tuning table (pyheat3d_b200.tune).
+    """
+    if kind not in _lib.VARIANT and kind != "auto":
         raise ValueError(f"unknown kind {kind!r}")
     if storage not in _lib.STORAGE:
         raise ValueError(f"unknown storage {storage!r}")

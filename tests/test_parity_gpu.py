@@ -252,7 +252,11 @@ def test_device_status_word_is_clear_after_runs():
 @pytest.mark.parametrize("bc", ["dirichlet", "periodic"])
 def test_every_compiled_config(storage, bc):
     """Every tile configuration in the tuning table gives the oracle's result."""
+    from pyheat3d_b200 import tune
+
     L = _lib.lib()
+    prev = tune.active_table()
+    tune.use(None)  # the steppers must not overwrite the configurations set here
     K = _lib.KERNEL
     S = _lib.STORAGE[storage]
     suf = {"float32": "", "bfloat16": "-bf16"}[storage]
@@ -272,3 +276,4 @@ def test_every_compiled_config(storage, bc):
     finally:
         for fam, k, _ in cases:
             L.ph3_tune_set(K[fam], 3, S, k, -1, 0)
+        tune.use(prev)

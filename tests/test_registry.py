@@ -25,7 +25,8 @@ def test_variant_table():
             v = VARIANTS[f"b200/tb{k}{suf}"]
             assert v.steps_per_pass == k and v.storage == st and v.dims == (2, 3)
     assert all(v.gpu and v.source and v.backend == "b200" for v in VARIANTS.values())
-    assert len(VARIANTS) == 3 * (3 + len(TB_KS))
+    assert len(VARIANTS) == 3 * (3 + len(TB_KS)) + 1
+    assert VARIANTS["b200/auto"].storage == "float32" and VARIANTS["b200/auto"].dims == (2, 3)
 
 
 def test_make_stepper_checks_dims_before_touching_the_gpu():

@@ -1,0 +1,56 @@
+"""Autotuner table: shape classes, persistence, nearest-class lookup, application (CPU)."""
+
+from __future__ import annotations
+
+import ctypes
+
+from pyheat3d_b200 import _lib, tune
+
+
+def test_shape_classes():
+    assert tune.shape_class(64 ** 3) == "small"
+    assert tune.shape_class(256 ** 3) == "medium"
+    assert tune.shape_class(512 ** 3) == "large"
+
+
+def test_table_roundtrip_and_lookup(tmp_path):
+    t = tune.Table({"gpu": "x"})
+    t.entries["zmarch:3:float32:1:large"] = {"cfg": 3, "chunk": 16, "glups": 1.0}
+    t.best["3:float32:large"] = {"k": 4, "variant": "tb", "glups": 2.0}
+    p = tmp_path / "t.json"
+    t.save(p)
+    u = tune.Table.load(p)
+    assert u.entry("zmarch", 3, "float32", 1, 512 ** 3)["cfg"] == 3
+    # nearest class: a small grid falls back to the large entry
+    assert u.entry("zmarch", 3, "float32", 1, 32 ** 3)["chunk"] == 16
+    assert u.entry("tb", 3, "float32", 4, 512 ** 3) is None
+    assert u.best_for(3, "float32", 100 ** 3)["k"] == 4
+
+
+def test_configure_writes_only_with_an_active_table():
+    L = _lib.lib()
+    K = _lib.KERNEL
+    cfg, chunk = ctypes.c_int(), ctypes.c_int()
+    prev = tune.active_table()
+    try:
+        _lib.check(L.ph3_tune_set(K["zmarch"], 3, 0, 1, 2, 24))
+        tune.use(None)
+        tune.configure(3, "float32", 1, 512 ** 3, L)
+        _lib.check(L.ph3_tune_get(K["zmarch"], 3, 0, 1, ctypes.byref(cfg), ctypes.byref(chunk)))
+        assert (cfg.value, chunk.value) == (2, 24)
+        t = tune.Table()
+        t.entries["zmarch:3:float32:1:large"] = {"cfg": 5, "chunk": 32, "glups": 1.0}
+        tune.use(t)
+        tune.configure(3, "float32", 1, 512 ** 3, L)
+        _lib.check(L.ph3_tune_get(K["zmarch"], 3, 0, 1, ctypes.byref(cfg), ctypes.byref(chunk)))
+        assert (cfg.value, chunk.value) == (5, 32)
+    finally:
+        L.ph3_tune_set(K["zmarch"], 3, 0, 1, -1, 0)
+        tune.use(prev)
+
+
+def test_batch_family_has_configurations():
+    L = _lib.lib()
+    n = L.ph3_tune_count(_lib.KERNEL["batch"], 3, 1)
+    assert n >= 2
+    assert all(L.ph3_tune_name(_lib.KERNEL["batch"], 3, 1, i) for i in range(n))
