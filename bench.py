@@ -67,9 +67,15 @@ def parse() -> argparse.Namespace:
                     help="length of the Poisson request stream (2000 req/s)")
     ap.add_argument("--variant", default="b200/zmarch",
                     help="kernel of the headline line (b200/zmarch; others for profiling)")
-    ap.add_argument("--n", type=int, default=N3,
-                    help="grid edge of the headline field (512; smaller only for profiling)")
-    return ap.parse_args()
+    ap.add_argument("--n", type=int, default=None,
+                    help="grid edge of the headline field (512; other sizes only for profiling)")
+    ap.add_argument("--dims", type=int, default=3, choices=(2, 3),
+                    help="3 (the headline); 2 runs a 2D n^2 field (n = 16384) for profiling "
+                         "the 2D kernels")
+    a = ap.parse_args()
+    if a.n is None:
+        a.n = N3 if a.dims == 3 else N2
+    return a
 
 
 # ---------------------------------------------------------------------------------------------
@@ -293,8 +299,8 @@ def run_b200(a: argparse.Namespace) -> None:
     T, K, W = a.time_steps, a.steps, max(3, a.warmup)
     hbm_peak, peak_kind = peaks()
     copy_bw = copy_bandwidth(torch)
-    stencil = heat_stencil(3, R3, "periodic")
-    u0 = field(a.n, 3, seed=rank)
+    stencil = heat_stencil(a.dims, R3 if a.dims == 3 else R2, "periodic")
+    u0 = field(a.n, a.dims, seed=rank)
     cells = u0.size
 
     # ---- value: K solves, field resident in HBM
@@ -393,15 +399,20 @@ def run_b200(a: argparse.Namespace) -> None:
             torch.cuda.empty_cache()
 
     if rank == 0:
-        traffic = profile_traffic("zmarch_tma_512cubed_fp32.md" if a.variant == "b200/zmarch" else "")
+        headline = (a.dims, a.n, a.variant) == (3, N3, "b200/zmarch")
+        traffic = profile_traffic("zmarch_tma_512cubed_fp32.md" if headline else "")
+        metric = "GLUPS (3D 512^3 fp32 periodic FTCS, single-step TMA z-march)"
+        if not headline:  # a profiling run
+            metric = f"GLUPS ({a.dims}D {a.n}^{a.dims} {var.storage} periodic FTCS, {a.variant})"
         line = {
-            "metric": "GLUPS (3D 512^3 fp32 periodic FTCS, single-step TMA z-march)",
+            "metric": metric,
             "value": round(value, 2), "kernel": a.variant, "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": round(secs / K * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"3D {a.n}^3 {var.storage} periodic heat, r=0.95/6, "
+            "config": {"workload": f"{a.dims}D {a.n}^{a.dims} {var.storage} periodic heat, "
+                                   f"r=0.95/{2 * a.dims}, "
                                    f"uniform[0,1) seed 0 (rank r: seed r), {a.variant}",
-                       "grid": [a.n, a.n, a.n], "bc": "periodic", "storage": var.storage,
+                       "grid": [a.n] * a.dims, "bc": "periodic", "storage": var.storage,
                        "time_steps_per_step": T, "units": "site updates (all cells)",
                        "l2": "inputs larger than L2 (512 MiB field vs 126 MB L2)",
                        "parallelism": f"replicas x{ws}"},

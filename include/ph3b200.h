@@ -188,6 +188,18 @@ int ph3_batch_launch(void* ws, int n, void* stream);
 int ph3_batch_run_static(const ph3_problem* problems, int n, void* stream);
 
 /*
+ * ph3_wait_flag: the bounded wait every persistent kernel of this library uses, run alone on
+ * `stream` by one thread: poll *flag (device memory, acquire ordering) until it reaches `target`
+ * or `spin_limit` polls (1 .. 4194304, each backing off about 0.25 us) have passed. A wait that
+ * runs out records code 2 (dependency timeout) in the status word (ph3_device_status) and the
+ * kernel returns, leaving the context usable. It is the host-visible check of the watchdog
+ * path: a test points it at a flag that nothing sets and reads the status back. No counterpart
+ * in the reference, whose only failure handling is on the host (registry.py:185-189
+ * availability(), benchmark.py:289-293).
+ */
+int ph3_wait_flag(const int* flag, int target, unsigned int spin_limit, void* stream);
+
+/*
  * Tuning table (no counterpart in the reference, whose tile constants are module globals that
  * bench/tune.py monkey-patches, cupy_backend.py:50-70). Every family has a few compiled tile
  * configurations; the table holds, per (kernel, dims, storage, k), the configuration index and

@@ -40,6 +40,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "ph3_batch_prepare": (_i, [_p, _i, _p, _i64, _p]),
     "ph3_batch_launch": (_i, [_p, _i, _p]),
     "ph3_batch_run_static": (_i, [_p, _i, _p]),
+    "ph3_wait_flag": (_i, [_p, _i, ctypes.c_uint, _p]),
     "ph3_tune_count": (_i, [_i, _i, _i]),
     "ph3_tune_name": (ctypes.c_char_p, [_i, _i, _i, _i]),
     "ph3_tune_set": (_i, [_i, _i, _i, _i, _i, _i]),
@@ -90,6 +91,10 @@ def check(rc: int) -> None:
     """Raise :class:`Ph3Error` for a nonzero return code."""
     if rc != 0:
         raise Ph3Error(rc, last_error())
+
+
+#: status-word codes (ph3_common.cuh DeviceError)
+STATUS = {"ok": 0, "mbarrier_timeout": 1, "dependency_timeout": 2, "stop_requested": 3}
 
 
 def device_status(clear: bool = True) -> int:

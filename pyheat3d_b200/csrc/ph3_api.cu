@@ -8,6 +8,7 @@
 #include <mutex>
 
 #include "../../include/ph3b200.h"
+#include "ph3_common.cuh"
 #include "ph3_internal.h"
 
 namespace ph3 {
@@ -183,6 +184,25 @@ int ph3_device_status(int* code, int clear) {
         if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
     }
     return PH3_OK;
+}
+
+namespace ph3 {
+__global__ void wait_flag_kernel(const int* flag, int target, uint32_t limit, int* err) {
+    if (threadIdx.x == 0) wait_flag_geq(flag, target, limit, err, nullptr);
+}
+}  // namespace ph3
+
+int ph3_wait_flag(const int* flag, int target, unsigned int spin_limit, void* stream) {
+    if (flag == nullptr) return fail(PH3_EINVAL, "flag must be non-null");
+    if (reinterpret_cast<uintptr_t>(flag) % alignof(int) != 0)
+        return fail(PH3_EINVAL, "flag must be 4-byte aligned");
+    if (spin_limit == 0 || spin_limit > kSpinLimit)
+        return fail(PH3_EINVAL, "spin_limit must be in [1, %u], got %u", kSpinLimit, spin_limit);
+    int* err = status_ptr();
+    if (err == nullptr) return fail(PH3_ECUDA, "no CUDA device / status word unavailable");
+    ph3::wait_flag_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(flag, target, spin_limit,
+                                                                       err);
+    return finish(cudaGetLastError(), "wait_flag launch");
 }
 
 int ph3_naive2d(const void* u, void* out, const float* src, int ny, int nx, float c0, float c1,

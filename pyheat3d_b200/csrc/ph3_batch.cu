@@ -81,12 +81,6 @@ __host__ __device__ __forceinline__ long long counter_bytes(int n) {
 }
 long long align256(long long x) { return ((x + 255) / 256) * 256; }
 
-__device__ __forceinline__ int ld_acquire(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 // Not inlined: each (storage, boundary, configuration) tile body keeps its own register
 // allocation instead of the kernel carrying the union of all of them.
 template <typename T, bool PER, int CFG>
@@ -161,16 +155,9 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
                 s_s = s;
                 s_t = int(j - tilepre[q]);
                 const int need = s * desc[p].ntiles;
-                uint32_t spins = 0;
-                while (ld_acquire(&done[p]) < need) {
-                    __nanosleep(spins < 64 ? 32 : 256);
-                    if (++spins > kSpinLimit ||
-                        *reinterpret_cast<volatile int*>(abort_flag) != 0) {
-                        record_error(err, kDevDependTimeout);
-                        atomicExch(abort_flag, 1);
-                        item = -1;
-                        break;
-                    }
+                if (!wait_flag_geq(&done[p], need, kSpinLimit, err, abort_flag)) {
+                    atomicExch(abort_flag, 1);
+                    item = -1;
                 }
                 __threadfence();
             }

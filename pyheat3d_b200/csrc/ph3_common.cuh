@@ -233,6 +233,29 @@ __device__ __forceinline__ void record_error(int* err, int code) {
 // well over a second of waiting before a wait is declared stuck.
 constexpr uint32_t kSpinLimit = 1u << 22;
 
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Bounded wait until *flag >= target (acquire ordering), backing off with __nanosleep. Gives up
+// after `limit` polls, or as soon as *abort (if given) is nonzero; a wait that gives up records
+// kDevDependTimeout in the status word and returns false.
+__device__ __forceinline__ bool wait_flag_geq(const int* flag, int target, uint32_t limit,
+                                              int* err, const int* abort) {
+    uint32_t spins = 0;
+    while (ld_acquire_gpu(flag) < target) {
+        __nanosleep(spins < 64 ? 32 : 256);
+        if (++spins > limit ||
+            (abort != nullptr && *reinterpret_cast<const volatile int*>(abort) != 0)) {
+            record_error(err, kDevDependTimeout);
+            return false;
+        }
+    }
+    return true;
+}
+
 // ------------------------------------------------------------------------------------------
 // mbarrier + TMA (cp.async.bulk) wrappers, written from the PTX ISA
 // ------------------------------------------------------------------------------------------

@@ -116,3 +116,11 @@ def test_tuning_table_roundtrip(lib):
     assert lib.ph3_tune_set(K["tb"], 3, 0, 4, 99, 0) == 1
     assert lib.ph3_tune_set(K["tb"], 4, 0, 4, 0, 0) == 1
     assert lib.ph3_tune_set(K["tb"], 3, 0, 4, 0, -5) == 1
+
+
+def test_wait_flag_rejects_bad_arguments(lib):
+    assert lib.ph3_wait_flag(None, 1, 16, None) == 1 and "non-null" in _lib.last_error()
+    assert lib.ph3_wait_flag(P(18), 1, 16, None) == 1 and "aligned" in _lib.last_error()
+    assert lib.ph3_wait_flag(P(16), 1, 0, None) == 1 and "spin_limit" in _lib.last_error()
+    assert lib.ph3_wait_flag(P(16), 1, (1 << 22) + 1, None) == 1
+    assert "spin_limit" in _lib.last_error()
