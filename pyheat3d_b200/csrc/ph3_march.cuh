@@ -185,6 +185,116 @@ __device__ __forceinline__ void march2d_item(const T* __restrict__ u, T* __restr
 }
 
 // ------------------------------------------------------------------------------------------
+// 2D single step, y-march with raw rows: the same walk as march2d_item, but each row of the
+// window and every prefetched row stays one 16-byte storage vector per lane (V = 16 / sizeof(T)
+// values) and is widened to fp32 only where it is used. A 16-bit row then costs 4 registers
+// instead of 8, so the same register budget keeps twice the rows (bytes) in flight. Requires
+// whole 16-byte row vectors (nx % V == 0, 16-byte aligned buffers).
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void widen16(const uint4& w, float (&v)[16 / sizeof(T)]) {
+    union { uint4 w; T e[16 / sizeof(T)]; } un;
+    un.w = w;
+#pragma unroll
+    for (int j = 0; j < int(16 / sizeof(T)); ++j) v[j] = to_f(un.e[j]);
+}
+template <bool CG>
+__device__ __forceinline__ uint4 ld16(const void* p) {
+    if constexpr (CG) return __ldcg(reinterpret_cast<const uint4*>(p));
+    else return __ldg(reinterpret_cast<const uint4*>(p));
+}
+
+template <typename T, bool PER, int RB, bool CG>
+__device__ __forceinline__ void march2d_raw_item(const T* __restrict__ u, T* __restrict__ o,
+                                                 const float* __restrict__ b, int ny, int nx,
+                                                 float c0, float c1, int strip, int cy, int ych) {
+    constexpr int V = 16 / int(sizeof(T));
+    constexpr int EX = 32 * V;
+    const int lane = threadIdx.x & 31;
+    const int x0 = strip * EX;
+    if (x0 >= nx) return;  // whole warp leaves together; no block-wide sync in this function
+    const int gx = x0 + lane * V;
+    int ylo = cy * ych, yhi = min(ylo + ych, ny);
+    if constexpr (!PER) { ylo = max(ylo, 1); yhi = min(yhi, ny - 1); }
+    if (ylo >= yhi) return;
+
+    // lanes past the last column read a wrapped (periodic) or clamped vector and store nothing;
+    // with periodic wrap the lane after column nx-1 then holds column 0, the right neighbour
+    const int base = PER ? wrap_idx(gx, nx) : clamp_idx(gx, 0, nx - V);
+    const int xl = fix_idx<PER>(x0 - 1, nx);
+    const int xr = fix_idx<PER>(x0 + EX, nx);
+    const bool writer = gx < nx;
+    uint32_t skip = 0;  // Dirichlet boundary columns are never written
+    if constexpr (!PER) {
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+            if (gx + j <= 0 || gx + j >= nx - 1) skip |= 1u << j;
+    }
+
+    uint4 win[RB + 2], pre[RB];
+    float hl[RB + 2], hr[RB + 2], pl[RB], pr[RB];
+    auto load_row = [&](int y, uint4& v, float& l, float& r) {
+        const T* row = u + int64_t(fix_idx<PER>(y, ny)) * nx;
+        v = ld16<CG>(row + base);
+        l = lane == 0 ? ldx1<CG>(row + xl) : 0.f;
+        r = lane == 31 ? ldx1<CG>(row + xr) : 0.f;
+    };
+#pragma unroll
+    for (int q = 0; q < RB + 2; ++q) load_row(ylo - 1 + q, win[q], hl[q], hr[q]);
+
+    for (int y = ylo; y < yhi; y += RB) {
+        const bool more = y + RB < yhi;
+        if (more) {
+#pragma unroll
+            for (int q = 0; q < RB; ++q) load_row(y + RB + 1 + q, pre[q], pl[q], pr[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < RB; ++q) {
+            const int yy = y + q;
+            if (yy >= yhi) break;
+            float c[V], m[V], p[V];
+            widen16<T>(win[q + 1], c);
+            widen16<T>(win[q], m);
+            widen16<T>(win[q + 2], p);
+            const float left = __shfl_up_sync(kFull, c[V - 1], 1);
+            const float right = __shfl_down_sync(kFull, c[0], 1);
+            float bv[V];
+            if (b != nullptr) ld_src<V>(b + int64_t(yy) * nx + base, true, bv);
+            float out[V];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                const float xm = j > 0 ? c[j - 1] : (lane == 0 ? hl[q + 1] : left);
+                const float xp = j < V - 1 ? c[j + 1] : (lane == 31 ? hr[q + 1] : right);
+                float v = upd2(c0, c1, c[j], xm, xp, m[j], p[j]);
+                if (b != nullptr) v = __fadd_rn(v, bv[j]);
+                out[j] = v;
+            }
+            if (writer) {
+                T* dst = o + int64_t(yy) * nx + gx;
+                if (skip == 0) {
+                    st_vec<T, V>(dst, out);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < V; ++j)
+                        if (!((skip >> j) & 1u)) dst[j] = from_f<T>(out[j]);
+                }
+            }
+        }
+        if (more) {
+            win[0] = win[RB];
+            win[1] = win[RB + 1];
+            hl[0] = hl[RB]; hl[1] = hl[RB + 1]; hr[0] = hr[RB]; hr[1] = hr[RB + 1];
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+                win[q + 2] = pre[q];
+                hl[q + 2] = pl[q];
+                hr[q + 2] = pr[q];
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // 3D single step, z-march with plain loads (any shape): the block owns an xy tile of 32*V x
 // W*R sites; warp w holds R rows, lane l holds V columns per row as one vector. The z-neighbours
 // form a register queue (below / centre / above) and the plane after `above` is in flight while

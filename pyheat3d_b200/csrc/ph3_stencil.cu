@@ -76,6 +76,14 @@ march2d_k1_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __res
                                           ych, vec_i != 0);
 }
 
+template <typename T, bool PER, int W, int RB>
+__global__ void __launch_bounds__(32 * W)
+march2d_raw_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b,
+                   int ny, int nx, float c0, float c1, int ych) {
+    march2d_raw_item<T, PER, RB, false>(u, o, b, ny, nx, c0, c1, blockIdx.x * W + (threadIdx.x >> 5),
+                                        blockIdx.y, ych);
+}
+
 template <typename T, bool PER, int V, int R, int W>
 __global__ void __launch_bounds__(32 * W)
 march3d_k1_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b,
@@ -397,6 +405,23 @@ static cudaError_t march_k1_t(const Launch& L) {
         }
         return cudaGetLastError();
     }
+    if (L.dims == 2 && cfg >= 2 && vec_ok<T, PER, 16 / sizeof(T)>(L)) {
+        // raw-row march: 2 -> 4 rows per step, 3 -> 8 rows per step (4 warps per block)
+        constexpr int V = 16 / sizeof(T), W = 4;
+        const int rb = cfg == 2 ? 4 : 8;
+        const int strips = cdiv(L.nx, 32 * V);
+        const int ych = L.chunk > 0 ? L.chunk
+                                    : default_chunk(L.ny, cdiv(strips, W), 4 * rb, target);
+        dim3 grd(cdiv(strips, W), cdiv(L.ny, ych));
+        if (grd.y > 65535) return cudaErrorInvalidConfiguration;
+        if (cfg == 2)
+            march2d_raw_kernel<T, PER, W, 4><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.ny, L.nx,
+                                                                         L.c0, L.c1, ych);
+        else
+            march2d_raw_kernel<T, PER, W, 8><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.ny, L.nx,
+                                                                         L.c0, L.c1, ych);
+        return cudaGetLastError();
+    }
     if (L.dims == 2) {
         constexpr int V = 16 / sizeof(T), W = 4, RB = sizeof(T) == 4 ? 4 : 2;
         const int strips = cdiv(L.nx, 32 * V);
@@ -489,10 +514,15 @@ cudaError_t launch_tb(const Launch& L) {
     return launch_tb_plain(L);
 }
 
+// 2D: 0 lean one-column-per-lane march, 1 float-window vector march, 2 / 3 raw-row vector march
+// with 4 / 8 rows per step (shapes without whole 16-byte rows fall back to 1). 3D: 0 lean, 1
+// vector march.
 int march_configs(int dims, const char** names, int max) {
-    if (names != nullptr && max > 0) names[0] = dims == 2 ? "lane1_W4_RB4" : "lane1_R4_W4";
-    if (names != nullptr && max > 1) names[1] = dims == 2 ? "V16B_W4_RB4" : "V16B_R2_W8";
-    return 2;
+    static const char* k2[] = {"lane1_W4_RB4", "V16B_W4_RB4", "raw16B_W4_RB4", "raw16B_W4_RB8"};
+    static const char* k3[] = {"lane1_R4_W4", "V16B_R2_W8"};
+    const int n = dims == 2 ? 4 : 2;
+    for (int i = 0; i < n && names != nullptr && i < max; ++i) names[i] = dims == 2 ? k2[i] : k3[i];
+    return n;
 }
 
 int tb_configs(int dims, int k, const char** names, int max) {

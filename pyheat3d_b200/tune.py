@@ -340,4 +340,8 @@ def main(argv: list[str] | None = None) -> int:
 
 
 if __name__ == "__main__":
-    sys.exit(main())
+    # Run the package's own module object: the steppers consult `pyheat3d_b200.tune` for the
+    # active table, so `use(None)` during a sweep must act on that module, not on __main__.
+    from pyheat3d_b200 import tune as _package_module
+
+    sys.exit(_package_module.main())

@@ -265,6 +265,11 @@ def test_every_compiled_config(storage, bc):
     st = heat_stencil(3, 0.95 / 6, bc)
     cases = [("zmarch", 1, "b200/zmarch" + suf)] + [("tb", k, f"b200/tb{k}" + suf)
                                                       for k in (2, 3, 4, 8)]
+    # the single-step register marches: 2D (aligned rows, partial strip) and 3D (unaligned)
+    u2 = rng.random((41, 1160), dtype=np.float32)
+    st2 = heat_stencil(2, 0.95 / 4, bc)
+    u3 = rng.random((13, 21, 97), dtype=np.float32)
+    marches = [(2, u2, st2, "b200/ymarch" + suf), (3, u3, st, "b200/zmarch" + suf)]
     try:
         for fam, k, key in cases:
             for cfg in range(L.ph3_tune_count(K[fam], 3, k)):
@@ -273,7 +278,14 @@ def test_every_compiled_config(storage, bc):
                     steps = 2 * k + 1
                     _assert_same(_run(key, u0, st, steps), _ref(key, u0, st, steps),
                                  (key, cfg, chunk))
+        for dims, u, stc, key in marches:
+            for cfg in range(L.ph3_tune_count(K["march"], dims, 1)):
+                for chunk in (0, 7):
+                    _lib.check(L.ph3_tune_set(K["march"], dims, S, 1, cfg, chunk))
+                    _assert_same(_run(key, u, stc, 5), _ref(key, u, stc, 5), (key, cfg, chunk))
     finally:
         for fam, k, _ in cases:
             L.ph3_tune_set(K[fam], 3, S, k, -1, 0)
+        for dims in (2, 3):
+            L.ph3_tune_set(K["march"], dims, S, 1, -1, 0)
         tune.use(prev)

@@ -4,6 +4,8 @@ from __future__ import annotations
 
 import ctypes
 
+import pytest
+
 from pyheat3d_b200 import _lib, tune
 
 
@@ -54,3 +56,17 @@ def test_batch_family_has_configurations():
     n = L.ph3_tune_count(_lib.KERNEL["batch"], 3, 1)
     assert n >= 2
     assert all(L.ph3_tune_name(_lib.KERNEL["batch"], 3, 1, i) for i in range(n))
+
+
+def test_module_entry_point_runs_the_package_module(monkeypatch):
+    """`python -m pyheat3d_b200.tune` must act on the module the steppers read the table from
+    (a sweep's `use(None)` on a separate __main__ copy would leave the table in force)."""
+    import runpy
+
+    import pyheat3d_b200.tune as t
+
+    called = []
+    monkeypatch.setattr(t, "main", lambda argv=None: called.append(argv) or 0)
+    with pytest.raises(SystemExit) as e:
+        runpy.run_module("pyheat3d_b200.tune", run_name="__main__")
+    assert e.value.code == 0 and called == [None]
