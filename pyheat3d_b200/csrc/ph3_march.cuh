@@ -221,8 +221,11 @@ __device__ __forceinline__ void march2d_raw_item(const T* __restrict__ u, T* __r
     // lanes past the last column read a wrapped (periodic) or clamped vector and store nothing;
     // with periodic wrap the lane after column nx-1 then holds column 0, the right neighbour
     const int base = PER ? wrap_idx(gx, nx) : clamp_idx(gx, 0, nx - V);
-    const int xl = fix_idx<PER>(x0 - 1, nx);
-    const int xr = fix_idx<PER>(x0 + EX, nx);
+    // the strip's halo columns: lane 0 keeps the left one, lane 31 the right one (one register
+    // per row serves both, since no lane needs both)
+    const T* hcol = lane == 0 ? u + fix_idx<PER>(x0 - 1, nx)
+                              : u + fix_idx<PER>(lane == 31 ? x0 + EX : x0, nx);
+    const bool edge = lane == 0 || lane == 31;
     const bool writer = gx < nx;
     uint32_t skip = 0;  // Dirichlet boundary columns are never written
     if constexpr (!PER) {
@@ -230,32 +233,36 @@ __device__ __forceinline__ void march2d_raw_item(const T* __restrict__ u, T* __r
         for (int j = 0; j < V; ++j)
             if (gx + j <= 0 || gx + j >= nx - 1) skip |= 1u << j;
     }
-
-    uint4 win[RB + 2], pre[RB];
-    float hl[RB + 2], hr[RB + 2], pl[RB], pr[RB];
-    auto load_row = [&](int y, uint4& v, float& l, float& r) {
-        const T* row = u + int64_t(fix_idx<PER>(y, ny)) * nx;
-        v = ld16<CG>(row + base);
-        l = lane == 0 ? ldx1<CG>(row + xl) : 0.f;
-        r = lane == 31 ? ldx1<CG>(row + xr) : 0.f;
+    auto load_row = [&](int y, uint4& v, float& h) {
+        const int64_t off = int64_t(fix_idx<PER>(y, ny)) * nx;
+        v = ld16<CG>(u + off + base);
+        h = edge ? ldx1<CG>(hcol + off) : 0.f;
     };
-#pragma unroll
-    for (int q = 0; q < RB + 2; ++q) load_row(ylo - 1 + q, win[q], hl[q], hr[q]);
 
-    for (int y = ylo; y < yhi; y += RB) {
+    // Two row windows used in turn: a step computes RB rows from window W (rows y-1 .. y+RB)
+    // while the next RB rows load straight into window N; only the two overlap rows, already
+    // in registers, are copied. Prefetched rows are never moved, so a step never waits for
+    // the loads it issued.
+    uint4 P[RB + 2], Q[RB + 2];
+    float Ph[RB + 2], Qh[RB + 2];
+#pragma unroll
+    for (int q = 0; q < RB + 2; ++q) load_row(ylo - 1 + q, P[q], Ph[q]);
+
+    auto step = [&](int y, uint4 (&W)[RB + 2], float (&Wh)[RB + 2], uint4 (&N)[RB + 2],
+                    float (&Nh)[RB + 2]) -> bool {
         const bool more = y + RB < yhi;
         if (more) {
 #pragma unroll
-            for (int q = 0; q < RB; ++q) load_row(y + RB + 1 + q, pre[q], pl[q], pr[q]);
+            for (int q = 0; q < RB; ++q) load_row(y + RB + 1 + q, N[q + 2], Nh[q + 2]);
         }
 #pragma unroll
         for (int q = 0; q < RB; ++q) {
             const int yy = y + q;
             if (yy >= yhi) break;
             float c[V], m[V], p[V];
-            widen16<T>(win[q + 1], c);
-            widen16<T>(win[q], m);
-            widen16<T>(win[q + 2], p);
+            widen16<T>(W[q + 1], c);
+            widen16<T>(W[q], m);
+            widen16<T>(W[q + 2], p);
             const float left = __shfl_up_sync(kFull, c[V - 1], 1);
             const float right = __shfl_down_sync(kFull, c[0], 1);
             float bv[V];
@@ -263,8 +270,8 @@ __device__ __forceinline__ void march2d_raw_item(const T* __restrict__ u, T* __r
             float out[V];
 #pragma unroll
             for (int j = 0; j < V; ++j) {
-                const float xm = j > 0 ? c[j - 1] : (lane == 0 ? hl[q + 1] : left);
-                const float xp = j < V - 1 ? c[j + 1] : (lane == 31 ? hr[q + 1] : right);
+                const float xm = j > 0 ? c[j - 1] : (lane == 0 ? Wh[q + 1] : left);
+                const float xp = j < V - 1 ? c[j + 1] : (lane == 31 ? Wh[q + 1] : right);
                 float v = upd2(c0, c1, c[j], xm, xp, m[j], p[j]);
                 if (b != nullptr) v = __fadd_rn(v, bv[j]);
                 out[j] = v;
@@ -281,16 +288,18 @@ __device__ __forceinline__ void march2d_raw_item(const T* __restrict__ u, T* __r
             }
         }
         if (more) {
-            win[0] = win[RB];
-            win[1] = win[RB + 1];
-            hl[0] = hl[RB]; hl[1] = hl[RB + 1]; hr[0] = hr[RB]; hr[1] = hr[RB + 1];
-#pragma unroll
-            for (int q = 0; q < RB; ++q) {
-                win[q + 2] = pre[q];
-                hl[q + 2] = pl[q];
-                hr[q + 2] = pr[q];
-            }
+            N[0] = W[RB];
+            N[1] = W[RB + 1];
+            Nh[0] = Wh[RB];
+            Nh[1] = Wh[RB + 1];
         }
+        return more;
+    };
+    for (int y = ylo;;) {
+        if (!step(y, P, Ph, Q, Qh)) break;
+        y += RB;
+        if (!step(y, Q, Qh, P, Ph)) break;
+        y += RB;
     }
 }
 
@@ -450,13 +459,16 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
     struct Plane {
         float v[R], h[R];  // own rows; halo column (lanes 0 / 31)
         float up, dn;      // rows above / below the warp's rows
+        float s[R];        // Jacobi source of the own rows (0 without a source)
     };
     auto load = [&](int z, Plane& p) {
-        const T* pl = u + int64_t(fix_idx<PER>(z, nz)) * P;
+        const int64_t zo = int64_t(fix_idx<PER>(z, nz)) * P;
+        const T* pl = u + zo;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             p.v[r] = ldx1<CG>(pl + roff[r] + cx);
             p.h[r] = hl ? ldx1<CG>(pl + roff[r] + hcol) : 0.f;
+            p.s[r] = b != nullptr ? __ldg(b + zo + roff[r] + cx) : 0.f;
         }
         p.up = ldx1<CG>(pl + uoff + cx);
         p.dn = ldx1<CG>(pl + doff + cx);
@@ -467,13 +479,15 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
 #pragma unroll
         for (int r = 0; r < R; ++r) bel[r] = ldx1<CG>(pl + roff[r] + cx);
     }
-    Plane ctr, abv, pre;
-    load(zlo, ctr);
-    load(zlo + 1, abv);
-    for (int z = zlo; z < zhi; ++z) {
+    // Three planes in turn (centre, above, in flight): the loop runs three planes per pass
+    // and the roles rotate by name, so a loaded plane is never copied and a plane step never
+    // waits for the load it issued.
+    Plane A, B, C;
+    load(zlo, A);
+    load(zlo + 1, B);
+    auto step = [&](int z, const Plane& ctr, const Plane& abv, Plane& pre) -> bool {
         const bool more = z + 1 < zhi;
         if (more) load(z + 2, pre);
-        const float* bpl = b != nullptr ? b + int64_t(z) * P : nullptr;
         T* opl = o + int64_t(z) * P;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -485,13 +499,17 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
             const float ym = r > 0 ? ctr.v[r - 1] : ctr.up;
             const float yp = r < R - 1 ? ctr.v[r + 1] : ctr.dn;
             float v = upd3(c0, c1, c, xm, xp, ym, yp, bel[r], abv.v[r]);
-            if (bpl != nullptr) v = __fadd_rn(v, __ldg(bpl + roff[r] + cx));
+            if (b != nullptr) v = __fadd_rn(v, ctr.s[r]);
             if (!xskip && !((yskip >> r) & 1u)) opl[roff[r] + x] = from_f<T>(v);
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) bel[r] = ctr.v[r];
-        ctr = abv;
-        if (more) abv = pre;
+        return more;
+    };
+    for (int z = zlo;;) {
+        if (!step(z++, A, B, C)) break;
+        if (!step(z++, B, C, A)) break;
+        if (!step(z++, C, A, B)) break;
     }
 }
 
@@ -509,23 +527,25 @@ __device__ __forceinline__ void lite2d_item(const T* __restrict__ u, T* __restri
     const bool hl = lane == 0 || lane == 31;
     bool xskip = x >= nx;
     if constexpr (!PER) xskip = xskip || x == 0 || x == nx - 1;
-    // window rows ylo-1 .. ylo+RB and their halo values; the next RB rows in flight
-    float win[RB + 2], wh[RB + 2], pre[RB], ph[RB];
+    // two row windows used in turn (rows y-1 .. y+RB and their halo values): the next RB rows
+    // load straight into the other window, so only the two overlap rows are ever copied
+    float P[RB + 2], Ph[RB + 2], Q[RB + 2], Qh[RB + 2];
     auto row = [&](int y) { return u + int64_t(fix_idx<PER>(y, ny)) * nx; };
 #pragma unroll
     for (int q = 0; q < RB + 2; ++q) {
         const T* rp = row(ylo - 1 + q);
-        win[q] = ldx1<CG>(rp + cx);
-        wh[q] = hl ? ldx1<CG>(rp + hcol) : 0.f;
+        P[q] = ldx1<CG>(rp + cx);
+        Ph[q] = hl ? ldx1<CG>(rp + hcol) : 0.f;
     }
-    for (int y = ylo; y < yhi; y += RB) {
+    auto step = [&](int y, const float (&win)[RB + 2], const float (&wh)[RB + 2],
+                    float (&N)[RB + 2], float (&Nh)[RB + 2]) -> bool {
         const bool more = y + RB < yhi;
         if (more) {
 #pragma unroll
             for (int q = 0; q < RB; ++q) {
                 const T* rp = row(y + RB + 1 + q);
-                pre[q] = ldx1<CG>(rp + cx);
-                ph[q] = hl ? ldx1<CG>(rp + hcol) : 0.f;
+                N[q + 2] = ldx1<CG>(rp + cx);
+                Nh[q + 2] = hl ? ldx1<CG>(rp + hcol) : 0.f;
             }
         }
 #pragma unroll
@@ -542,14 +562,16 @@ __device__ __forceinline__ void lite2d_item(const T* __restrict__ u, T* __restri
             if (!xskip) o[int64_t(yy) * nx + x] = from_f<T>(v);
         }
         if (more) {
-            win[0] = win[RB]; wh[0] = wh[RB];
-            win[1] = win[RB + 1]; wh[1] = wh[RB + 1];
-#pragma unroll
-            for (int q = 0; q < RB; ++q) {
-                win[q + 2] = pre[q];
-                wh[q + 2] = ph[q];
-            }
+            N[0] = win[RB]; Nh[0] = wh[RB];
+            N[1] = win[RB + 1]; Nh[1] = wh[RB + 1];
         }
+        return more;
+    };
+    for (int y = ylo;;) {
+        if (!step(y, P, Ph, Q, Qh)) break;
+        y += RB;
+        if (!step(y, Q, Qh, P, Ph)) break;
+        y += RB;
     }
 }
 

@@ -381,9 +381,10 @@ static cudaError_t march_k1_t(const Launch& L) {
     const T* u = static_cast<const T*>(L.u);
     T* o = static_cast<T*>(L.out);
     const long long target = 8LL * sm_count();
-    // default: lean one-column-per-lane march in 3D (2.1-2.4x the vector march on unaligned
-    // grids on a B200), the vector march in 2D (1.3-1.4x the lean one)
-    const int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : 1);
+    // defaults measured on a B200: in 3D the lean one-column-per-lane march (2.1-2.4x the
+    // vector march on unaligned grids); in 2D the raw-row march with 8 rows per step (16384^2:
+    // fp32 805 vs 674 GLUPS for the float-window march, bf16 1257 vs 547)
+    const int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : 3);
     if (cfg == 0) {
         if (L.dims == 2) {
             constexpr int W = 4, RB = 4;
@@ -410,8 +411,10 @@ static cudaError_t march_k1_t(const Launch& L) {
         constexpr int V = 16 / sizeof(T), W = 4;
         const int rb = cfg == 2 ? 4 : 8;
         const int strips = cdiv(L.nx, 32 * V);
+        // many short row chunks (about 64 rows at 16384^2, the measured best) keep more blocks
+        // and loads in flight than one chunk per resident block
         const int ych = L.chunk > 0 ? L.chunk
-                                    : default_chunk(L.ny, cdiv(strips, W), 4 * rb, target);
+                                    : default_chunk(L.ny, cdiv(strips, W), 4 * rb, 8 * target);
         dim3 grd(cdiv(strips, W), cdiv(L.ny, ych));
         if (grd.y > 65535) return cudaErrorInvalidConfiguration;
         if (cfg == 2)

@@ -97,10 +97,7 @@ __device__ __forceinline__ void stg_lane(T* p, const float2 (&v)[V / 2]) {
     st_vec<T, V>(p, f);
 }
 
-// LEAN: the x-neighbour sums are formed by scalar adds straight into register pairs (no pair
-// shuffling moves) and the plane loop runs two planes per iteration with the two per-level
-// plane arrays swapping roles, so only one register copy per value and level remains.
-template <typename T, bool PER, int K, int V, int R, int NWC, int STAGES, bool LEAN>
+template <typename T, bool PER, int K, int V, int R, int NWC, int STAGES>
 __global__ void __launch_bounds__(32 * NWC, 1)
 tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b,
                  TbGeom g, float c0, float c1, int* err) {
@@ -210,7 +207,7 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
 #pragma unroll
                 for (int p = 0; p < NP; ++p) A[s][r][p] = B[s][r][p] = make_float2(0.f, 0.f);
 
-        auto step = [&](int iz, float2 (&Bp)[K][R][NP], float2 (&Ap)[K][R][NP]) {
+        for (int iz = z0 - K; iz < z1 + K; ++iz, ++it) {
             if (ok) issue_next();
             const int s = it % STAGES;
             if (ok) {
@@ -234,21 +231,21 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 const int c = iz - lev;
                 // y-neighbours of the first / last row: exchange with the adjacent warps
                 float* eb = edge + buf * (2 * NWC * EX);
-                put_lane<NP>(eb + warp * EX + lx, Ap[lev - 1][0]);
-                put_lane<NP>(eb + (NWC + warp) * EX + lx, Ap[lev - 1][R - 1]);
+                put_lane<NP>(eb + warp * EX + lx, A[lev - 1][0]);
+                put_lane<NP>(eb + (NWC + warp) * EX + lx, A[lev - 1][R - 1]);
                 named_sync(1, NWC * 32);
                 float2 up[NP], dn[NP];
                 if (warp > 0) {
                     get_lane<NP>(eb + (NWC + warp - 1) * EX + lx, up);
                 } else {
 #pragma unroll
-                    for (int p = 0; p < NP; ++p) up[p] = Ap[lev - 1][0][p];
+                    for (int p = 0; p < NP; ++p) up[p] = A[lev - 1][0][p];
                 }
                 if (warp < NWC - 1) {
                     get_lane<NP>(eb + (warp + 1) * EX + lx, dn);
                 } else {
 #pragma unroll
-                    for (int p = 0; p < NP; ++p) dn[p] = Ap[lev - 1][R - 1][p];
+                    for (int p = 0; p < NP; ++p) dn[p] = A[lev - 1][R - 1][p];
                 }
                 buf ^= 1;
                 const bool zfix = !PER && (c <= 0 || c >= g.nz - 1);
@@ -258,8 +255,8 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 float2 res[R][NP];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const float left = __shfl_up_sync(kFull, Ap[lev - 1][r][NP - 1].y, 1);
-                    const float right = __shfl_down_sync(kFull, Ap[lev - 1][r][0].x, 1);
+                    const float left = __shfl_up_sync(kFull, A[lev - 1][r][NP - 1].y, 1);
+                    const float right = __shfl_down_sync(kFull, A[lev - 1][r][0].x, 1);
                     float2 bv[NP];
                     if (bpl != nullptr) {
                         const int gy = PER ? wrap_idx(gy0 + r, g.ny) : clamp_idx(gy0 + r, 0, g.ny - 1);
@@ -270,20 +267,12 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                     }
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
-                        const float2 ctr = Ap[lev - 1][r][p];
-                        const float xl = p > 0 ? Ap[lev - 1][r][p - 1].y : left;
-                        const float xr = p < NP - 1 ? Ap[lev - 1][r][p + 1].x : right;
-                        const float2 ym = r > 0 ? Ap[lev - 1][r - 1][p] : up[p];
-                        const float2 yp = r < R - 1 ? Ap[lev - 1][r + 1][p] : dn[p];
-                        float2 v;
-                        if constexpr (LEAN) {
-                            const float2 sx = make_float2(__fadd_rn(xl, ctr.y), __fadd_rn(ctr.x, xr));
-                            v = upd3_sx2(c0v, c1v, ctr, sx, ym, yp, Bp[lev - 1][r][p], N[r][p]);
-                        } else {
-                            const float2 xm = make_float2(xl, ctr.x);
-                            const float2 xp = make_float2(ctr.y, xr);
-                            v = upd3_x2(c0v, c1v, ctr, xm, xp, ym, yp, Bp[lev - 1][r][p], N[r][p]);
-                        }
+                        const float2 ctr = A[lev - 1][r][p];
+                        const float2 xm = make_float2(p > 0 ? A[lev - 1][r][p - 1].y : left, ctr.x);
+                        const float2 xp = make_float2(ctr.y, p < NP - 1 ? A[lev - 1][r][p + 1].x : right);
+                        const float2 ym = r > 0 ? A[lev - 1][r - 1][p] : up[p];
+                        const float2 yp = r < R - 1 ? A[lev - 1][r + 1][p] : dn[p];
+                        float2 v = upd3_x2(c0v, c1v, ctr, xm, xp, ym, yp, B[lev - 1][r][p], N[r][p]);
                         if (bpl != nullptr) v = add2(v, bv[p]);
                         if constexpr (!PER) {
                             const bool fr = zfix || ((fixy >> r) & 1u);
@@ -297,13 +286,8 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 for (int r = 0; r < R; ++r)
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
-                        if constexpr (LEAN) {
-                            // the caller swaps the arrays: Ap becomes plane c-1, Bp plane c
-                            Bp[lev - 1][r][p] = N[r][p];
-                        } else {
-                            Bp[lev - 1][r][p] = Ap[lev - 1][r][p];
-                            Ap[lev - 1][r][p] = N[r][p];
-                        }
+                        B[lev - 1][r][p] = A[lev - 1][r][p];
+                        A[lev - 1][r][p] = N[r][p];
                         N[r][p] = res[r][p];
                     }
             }
@@ -328,15 +312,6 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                     }
                 }
             }
-            ++it;
-        };
-        if constexpr (LEAN) {
-            for (int iz = z0 - K; iz < z1 + K; iz += 2) {
-                step(iz, B, A);
-                if (iz + 1 < z1 + K) step(iz + 1, A, B);
-            }
-        } else {
-            for (int iz = z0 - K; iz < z1 + K; ++iz) step(iz, B, A);
         }
     }
 
@@ -370,10 +345,10 @@ int balanced_chunk(int nz, long long tiles, long long blocks, int k) {
     return best;
 }
 
-template <typename T, bool PER, int K, int V, int R, int NWC, int STAGES, bool LEAN = false>
+template <typename T, bool PER, int K, int V, int R, int NWC, int STAGES>
 cudaError_t tbbulk_t(const Launch& L) {
     using C = TbCfg<T, K, V, R, NWC, STAGES>;
-    auto kern = tb3d_bulk_kernel<T, PER, K, V, R, NWC, STAGES, LEAN>;
+    auto kern = tb3d_bulk_kernel<T, PER, K, V, R, NWC, STAGES>;
     static int blocks_per_sm[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -412,10 +387,8 @@ struct TbEntry {
     const char* name;
 };
 const TbEntry kTbNames[] = {
-    {2, "V4_R2_W16_S4"}, {2, "V4_R4_W8_S4"},  {2, "V4_R2_W16_S4_lean"}, {2, "V4_R4_W8_S4_lean"},
-    {3, "V4_R2_W16_S4"}, {3, "V4_R4_W8_S4"},  {3, "V4_R2_W16_S4_lean"}, {3, "V4_R4_W8_S4_lean"},
-    {4, "V4_R2_W16_S4"}, {4, "V2_R2_W16_S6"}, {4, "V4_R2_W16_S4_lean"}, {4, "V4_R4_W8_S4_lean"},
-    {8, "V2_R2_W16_S6"}, {8, "V2_R4_W8_S6"},  {8, "V2_R2_W16_S6_lean"}, {8, "V2_R4_W8_S6_lean"},
+    {2, "V4_R2_W16_S4"}, {2, "V4_R4_W8_S4"},  {3, "V4_R2_W16_S4"}, {3, "V4_R4_W8_S4"},
+    {4, "V4_R2_W16_S4"}, {4, "V2_R2_W16_S6"}, {8, "V2_R2_W16_S6"}, {8, "V2_R4_W8_S6"},
 };
 
 template <typename T, bool PER>
@@ -423,33 +396,13 @@ cudaError_t tbbulk_dispatch(const Launch& L) {
     const int cfg = L.cfg < 0 ? 0 : L.cfg;
     switch (L.k) {
         case 2:
-            switch (cfg) {
-                case 1: return tbbulk_t<T, PER, 2, 4, 4, 8, 4>(L);
-                case 2: return tbbulk_t<T, PER, 2, 4, 2, 16, 4, true>(L);
-                case 3: return tbbulk_t<T, PER, 2, 4, 4, 8, 4, true>(L);
-                default: return tbbulk_t<T, PER, 2, 4, 2, 16, 4>(L);
-            }
+            return cfg == 1 ? tbbulk_t<T, PER, 2, 4, 4, 8, 4>(L) : tbbulk_t<T, PER, 2, 4, 2, 16, 4>(L);
         case 3:
-            switch (cfg) {
-                case 1: return tbbulk_t<T, PER, 3, 4, 4, 8, 4>(L);
-                case 2: return tbbulk_t<T, PER, 3, 4, 2, 16, 4, true>(L);
-                case 3: return tbbulk_t<T, PER, 3, 4, 4, 8, 4, true>(L);
-                default: return tbbulk_t<T, PER, 3, 4, 2, 16, 4>(L);
-            }
+            return cfg == 1 ? tbbulk_t<T, PER, 3, 4, 4, 8, 4>(L) : tbbulk_t<T, PER, 3, 4, 2, 16, 4>(L);
         case 4:
-            switch (cfg) {
-                case 1: return tbbulk_t<T, PER, 4, 2, 2, 16, 6>(L);
-                case 2: return tbbulk_t<T, PER, 4, 4, 2, 16, 4, true>(L);
-                case 3: return tbbulk_t<T, PER, 4, 4, 4, 8, 4, true>(L);
-                default: return tbbulk_t<T, PER, 4, 4, 2, 16, 4>(L);
-            }
+            return cfg == 1 ? tbbulk_t<T, PER, 4, 2, 2, 16, 6>(L) : tbbulk_t<T, PER, 4, 4, 2, 16, 4>(L);
         case 8:
-            switch (cfg) {
-                case 1: return tbbulk_t<T, PER, 8, 2, 4, 8, 6>(L);
-                case 2: return tbbulk_t<T, PER, 8, 2, 2, 16, 6, true>(L);
-                case 3: return tbbulk_t<T, PER, 8, 2, 4, 8, 6, true>(L);
-                default: return tbbulk_t<T, PER, 8, 2, 2, 16, 6>(L);
-            }
+            return cfg == 1 ? tbbulk_t<T, PER, 8, 2, 4, 8, 6>(L) : tbbulk_t<T, PER, 8, 2, 2, 16, 6>(L);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -57,6 +57,21 @@ struct ZmGeom {
     int nitems;
 };
 
+// One lane's source values of one plane (RW rows x V fp32 values, as float4s). The consumers
+// load them one plane ahead, so the Jacobi source never stalls a plane on DRAM latency.
+template <int RW, int V>
+struct SrcRows {
+    float4 v[RW][V / 4];
+    __device__ __forceinline__ void load(const float* __restrict__ b, int64_t zoff,
+                                         const int (&boff)[RW]) {
+#pragma unroll
+        for (int r = 0; r < RW; ++r)
+#pragma unroll
+            for (int q = 0; q < V / 4; ++q)
+                v[r][q] = __ldg(reinterpret_cast<const float4*>(b + zoff + boff[r]) + q);
+    }
+};
+
 // Blocks per SM the register budget is sized for (the ring's shared memory allows as many).
 template <typename T, int TY, int NWC>
 constexpr int zm_min_blocks() {
@@ -200,6 +215,12 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
             if (rr >= 0 && rr < RW) wrap_r = rr;
         }
         float2 bel[RW][NP], ctr[RW][NP], abv[RW][NP];
+        int boff[RW];  // source offsets of the warp's rows within a plane
+#pragma unroll
+        for (int r = 0; r < RW; ++r)
+            boff[r] = min(y0 + r0 + r, g.ny - 1) * g.nx + min(gx, g.nx - V);
+        SrcRows<RW, V> bnext;
+        if (b != nullptr) bnext.load(b, int64_t(zlo) * P, boff);
 
         // plane zlo-1: only the own values are needed
         {
@@ -225,6 +246,11 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
             if (!mbar_wait(&full[sa], pha, err)) { ok = false; break; }
 #pragma unroll
             for (int r = 0; r < RW; ++r) PK::unpack(*stage_row(sa, r0 + r + 1), abv[r]);
+            SrcRows<RW, V> bcur;
+            if (b != nullptr) {
+                bcur = bnext;
+                if (z + 1 < zhi) bnext.load(b, int64_t(z + 1) * P, boff);
+            }
             // y-neighbours of the warp's first and last rows come from the staged centre plane
             float2 up[NP], dn[NP], wdn[NP];
             PK::unpack(*stage_row(sc, r0), up);
@@ -241,11 +267,9 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                 const float xrv = (lane == 31 || wrapx) ? to_f(sr[(r0 + r) * HX]) : right;
                 float2 bv[NP];
                 if (b != nullptr) {
-                    const float4* bp = reinterpret_cast<const float4*>(
-                        b + int64_t(z) * P + int64_t(min(gy, g.ny - 1)) * g.nx + min(gx, g.nx - V));
 #pragma unroll
                     for (int q = 0; q < NP / 2; ++q) {
-                        const float4 t4 = __ldg(bp + q);
+                        const float4 t4 = bcur.v[r][q];
                         bv[2 * q] = make_float2(t4.x, t4.y);
                         bv[2 * q + 1] = make_float2(t4.z, t4.w);
                     }
@@ -400,6 +424,12 @@ zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
         // halo loaded from column 0 / row 0
         const bool wrapx = PER && (gx + V == g.nx) && lane != 31;
         float bel[RW][V], ctr[RW][V], abv[RW][V];
+        int boff[RW];  // source offsets of the warp's rows within a plane
+#pragma unroll
+        for (int r = 0; r < RW; ++r)
+            boff[r] = min(y0 + r0 + r, g.ny - 1) * g.nx + min(gx, g.nx - V);
+        SrcRows<RW, V> bnext;
+        if (b != nullptr) bnext.load(b, int64_t(zlo) * P, boff);
 
         // plane zlo-1: only the own values are needed
         {
@@ -421,6 +451,11 @@ zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
             if (!mbar_wait(&full[sa], (it / STAGES) & 1u, err)) { ok = false; break; }
 #pragma unroll
             for (int r = 0; r < RW; ++r) lds_vec(body_row(sa, r0 + r + 1) + lane * V, abv[r]);
+            SrcRows<RW, V> bcur;
+            if (b != nullptr) {
+                bcur = bnext;
+                if (z + 1 < zhi) bnext.load(b, int64_t(z + 1) * P, boff);
+            }
             // y-neighbours of the first and last rows come from the staged centre plane
             // periodic partial tile: the row after ny-1 is the halo row loaded from row 0
             int wrap_r = -1;
@@ -444,11 +479,9 @@ zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
                 if (lane == 31 || wrapx) hr = to_f(sr[(r0 + r) * HX]);
                 float bv[V];
                 if (b != nullptr) {
-                    const float* bp = b + int64_t(z) * P + int64_t(min(gy, g.ny - 1)) * g.nx +
-                                      min(gx, g.nx - V);
 #pragma unroll
                     for (int q = 0; q < V / 4; ++q) {
-                        const float4 t = __ldg(reinterpret_cast<const float4*>(bp) + q);
+                        const float4 t = bcur.v[r][q];
                         bv[4 * q] = t.x; bv[4 * q + 1] = t.y; bv[4 * q + 2] = t.z; bv[4 * q + 3] = t.w;
                     }
                 }
@@ -503,218 +536,6 @@ zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
     }
 }
 
-// Second form of the consumer: the dataflow of the first with less work per plane. The z
-// register queue rotates by unrolling the plane loop three times (no register moves), the ring
-// stage and its phase advance by increments instead of divisions, the global row pointers move
-// by one plane, and with PACKED the neighbour sums run as f32x2 pairs (same rounding).
-template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED>
-__global__ void __launch_bounds__(32 * (NWC + 1), zm_min_blocks<T, TY, NWC>())
-zmarch_v2_kernel(const __grid_constant__ CUtensorMap tm_body,
-                 const __grid_constant__ CUtensorMap tm_row,
-                 const __grid_constant__ CUtensorMap tm_side, T* __restrict__ o,
-                 const float* __restrict__ b, ZmGeom g, float c0, float c1, int* err) {
-    using C = ZmCfg<T, TY, NWC, STAGES>;
-    constexpr int V = C::V, TX = C::TX, HX = C::HX, RW = C::RW;
-    constexpr int ROW_BYTES = TX * int(sizeof(T));
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE_BYTES);
-    uint64_t* empty = full + STAGES;
-    volatile int* issued = reinterpret_cast<volatile int*>(empty + STAGES);
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], NWC);
-        }
-        *issued = 0;
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    if (warp == NWC) {
-        if (lane == 0)
-            zm_produce<T, PER, TY, NWC, STAGES>(&tm_body, &tm_row, &tm_side, g, smem, full,
-                                                empty, issued, err);
-        return;
-    }
-
-    // --------------------------------------------------------------------- consumer warps
-    const int64_t P = int64_t(g.nx) * g.ny;
-    const int r0 = warp * RW;   // first tile row of this warp
-    int s = 0;                  // stage of the next plane to take
-    uint32_t ph = 0;            // its full-barrier parity
-    uint32_t taken = 0;         // planes taken so far (the drain starts there)
-    bool ok = true;
-    const unsigned char* lane_base = smem + lane * 16;  // this lane's 16 bytes of a staged row
-    auto row_vec = [&](int st, int row, float (&v)[V]) {
-        union { uint4 w; T e[V]; } un;
-        un.w = *reinterpret_cast<const uint4*>(lane_base + st * C::STAGE_BYTES + row * ROW_BYTES);
-#pragma unroll
-        for (int j = 0; j < V; ++j) v[j] = to_f(un.e[j]);
-    };
-    auto side_val = [&](int st, int right, int idx) -> float {
-        return to_f(reinterpret_cast<const T*>(smem + st * C::STAGE_BYTES + C::BODY_BYTES +
-                                               right * C::SIDE_BYTES)[idx]);
-    };
-    auto advance = [&]() {
-        if (++s == STAGES) { s = 0; ph ^= 1u; }
-        ++taken;
-    };
-    auto release = [&](int st) {
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[st]);
-    };
-    const float2 c0v = make_float2(c0, c0), c1v = make_float2(c1, c1);
-
-    for (int item = blockIdx.x; item < g.nitems && ok; item += gridDim.x) {
-        const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty;
-        const int ch = item / (g.ntx * g.nty);
-        const int x0 = tx * TX, y0 = ty * TY;
-        const int zlo = g.zbase + ch * g.zch;
-        const int zhi = min(zlo + g.zch, g.zbase + g.nzi);
-        const int gx = x0 + lane * V;
-        uint32_t skipx = 0, skipy = 0;  // sites this thread must not write
-#pragma unroll
-        for (int j = 0; j < V; ++j)
-            if (gx + j >= g.nx || (!PER && (gx + j == 0 || gx + j == g.nx - 1))) skipx |= 1u << j;
-#pragma unroll
-        for (int r = 0; r < RW; ++r) {
-            const int gy = y0 + r0 + r;
-            if (gy >= g.ny || (!PER && (gy == 0 || gy == g.ny - 1))) skipy |= 1u << r;
-        }
-        // periodic wrap inside a partial tile: the site after column nx-1 / row ny-1 is the
-        // halo loaded from column 0 / row 0
-        const bool wrapx = PER && (gx + V == g.nx) && lane != 31;
-        const bool right_halo = lane == 31 || wrapx;
-        int wrap_r = -1;
-        if (PER && y0 + TY > g.ny) {
-            const int rr = g.ny - 1 - (y0 + r0);
-            if (rr >= 0 && rr < RW) wrap_r = rr;
-        }
-        const int dn_row = wrap_r == RW - 1 ? TY + 1 : r0 + RW + 1;
-        T* dst = o + int64_t(zlo) * P + int64_t(y0 + r0) * g.nx + gx;  // row r0 of plane z
-        const float* bz = b != nullptr ? b + int64_t(zlo) * P : nullptr;
-        int boff[RW];
-#pragma unroll
-        for (int r = 0; r < RW; ++r)
-            boff[r] = min(y0 + r0 + r, g.ny - 1) * g.nx + min(gx, g.nx - V);
-
-        float qa[RW][V], qb[RW][V], qc[RW][V];
-        // plane zlo-1 (only the own rows are needed)
-        if (!mbar_wait(&full[s], ph, err)) { ok = false; break; }
-#pragma unroll
-        for (int r = 0; r < RW; ++r) row_vec(s, r0 + r + 1, qa[r]);
-        release(s);
-        advance();
-        // plane zlo: the first centre plane, its stage stays held
-        int sc = s;
-        if (!mbar_wait(&full[s], ph, err)) { ok = false; break; }
-#pragma unroll
-        for (int r = 0; r < RW; ++r) row_vec(s, r0 + r + 1, qb[r]);
-        advance();
-
-        auto plane = [&](float (&bel)[RW][V], float (&ctr)[RW][V], float (&abv)[RW][V]) -> bool {
-            if (!mbar_wait(&full[s], ph, err)) return false;
-#pragma unroll
-            for (int r = 0; r < RW; ++r) row_vec(s, r0 + r + 1, abv[r]);
-            float up[V], dn[V], wdn[V];
-            row_vec(sc, r0, up);
-            row_vec(sc, dn_row, dn);
-            if (wrap_r >= 0 && wrap_r < RW - 1) row_vec(sc, TY + 1, wdn);
-#pragma unroll
-            for (int r = 0; r < RW; ++r) {
-                const float left = __shfl_up_sync(kFullMask, ctr[r][V - 1], 1);
-                const float right = __shfl_down_sync(kFullMask, ctr[r][0], 1);
-                const float xlv = lane == 0 ? side_val(sc, 0, (r0 + r) * HX + HX - 1) : left;
-                const float xrv = right_halo ? side_val(sc, 1, (r0 + r) * HX) : right;
-                float bv[V];
-                if (bz != nullptr) {
-                    const float4* bp = reinterpret_cast<const float4*>(bz + boff[r]);
-#pragma unroll
-                    for (int q = 0; q < V / 4; ++q) {
-                        const float4 t4 = __ldg(bp + q);
-                        bv[4 * q] = t4.x; bv[4 * q + 1] = t4.y;
-                        bv[4 * q + 2] = t4.z; bv[4 * q + 3] = t4.w;
-                    }
-                }
-                float out[V];
-#pragma unroll
-                for (int j = 0; j < V; j += 2) {
-                    const float xm0 = j > 0 ? ctr[r][j - 1] : xlv;
-                    const float xp1 = j + 2 < V ? ctr[r][j + 2] : xrv;
-                    float ym[2], yp[2];
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        ym[e] = r > 0 ? ctr[r - 1][j + e] : up[j + e];
-                        yp[e] = dn[j + e];
-                        if (r < RW - 1) yp[e] = r == wrap_r ? wdn[j + e] : ctr[r + 1][j + e];
-                    }
-                    if constexpr (PACKED) {
-                        const float2 sx = make_float2(__fadd_rn(xm0, ctr[r][j + 1]),
-                                                      __fadd_rn(ctr[r][j], xp1));
-                        float2 v = upd3_sx2(c0v, c1v, make_float2(ctr[r][j], ctr[r][j + 1]), sx,
-                                            make_float2(ym[0], ym[1]), make_float2(yp[0], yp[1]),
-                                            make_float2(bel[r][j], bel[r][j + 1]),
-                                            make_float2(abv[r][j], abv[r][j + 1]));
-                        if (bz != nullptr) v = add2(v, make_float2(bv[j], bv[j + 1]));
-                        out[j] = v.x;
-                        out[j + 1] = v.y;
-                    } else {
-                        out[j] = upd3(c0, c1, ctr[r][j], xm0, ctr[r][j + 1], ym[0], yp[0],
-                                      bel[r][j], abv[r][j]);
-                        out[j + 1] = upd3(c0, c1, ctr[r][j + 1], ctr[r][j], xp1, ym[1], yp[1],
-                                          bel[r][j + 1], abv[r][j + 1]);
-                        if (bz != nullptr) {
-                            out[j] = __fadd_rn(out[j], bv[j]);
-                            out[j + 1] = __fadd_rn(out[j + 1], bv[j + 1]);
-                        }
-                    }
-                }
-                if (!((skipy >> r) & 1u)) {
-                    T* d = dst + r * g.nx;
-                    if (skipx == 0) {
-                        st_vec<T, V>(d, out);
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < V; ++j)
-                            if (!((skipx >> j) & 1u)) d[j] = from_f<T>(out[j]);
-                    }
-                }
-            }
-            release(sc);
-            sc = s;
-            advance();
-            dst += P;
-            if (bz != nullptr) bz += P;
-            return true;
-        };
-        int z = zlo;
-        for (;;) {
-            if (z >= zhi) break;
-            if (!plane(qa, qb, qc)) { ok = false; break; }
-            if (++z >= zhi) break;
-            if (!plane(qb, qc, qa)) { ok = false; break; }
-            if (++z >= zhi) break;
-            if (!plane(qc, qa, qb)) { ok = false; break; }
-            ++z;
-        }
-        if (!ok) break;
-        release(sc);  // plane zhi
-    }
-
-    if (!ok) {
-        // a wait expired: drain the loads this block issued so no copy lands after exit
-        if (warp == 0 && lane == 0) {
-            const int n_issued = *issued;
-            for (int k = int(taken); k < n_issued; ++k) {
-                const int st = k % STAGES;
-                if (!mbar_wait(&full[st], (uint32_t(k) / STAGES) & 1u, err)) break;
-            }
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
@@ -753,14 +574,12 @@ bool make_map(CUtensorMap* m, const void* base, int nz, int ny, int nx, int bx, 
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// FORM: 0 the register-capped packed/scalar consumer, 1 the first scalar consumer, 2 the
-// second consumer (PACKED selects its f32x2 sums).
+// FORM: 0 the register-capped packed/scalar consumer, 1 the first scalar consumer.
 template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED = true, int FORM = 0>
 cudaError_t zmarch_t(const Launch& L) {
     using C = ZmCfg<T, TY, NWC, STAGES>;
     auto pick = [] {
         if constexpr (FORM == 1) return zmarch_v1_kernel<T, PER, TY, NWC, STAGES>;
-        else if constexpr (FORM == 2) return zmarch_v2_kernel<T, PER, TY, NWC, STAGES, PACKED>;
         else return zmarch_tma_kernel<T, PER, TY, NWC, STAGES, PACKED>;
     };
     auto kern = pick();
@@ -827,10 +646,8 @@ bool zmarch_tma_supported(const Launch& L) {
 // Compiled z-march configurations: rows per tile (TY), consumer warps (NWC), ring stages.
 static const char* kZmNames[] = {"TY16_W8_S6", "TY8_W8_S8", "TY32_W8_S4", "TY16_W16_S6",
                                  "TY8_W4_S8", "TY16_W8_S6_scalar", "TY16_W16_S6_scalar",
-                                 "TY16_W8_S6_v1", "TY16_W16_S6_v1", "TY16_W16_S6_v2",
-                                 "TY16_W16_S6_v2p", "TY32_W16_S6_v2", "TY16_W8_S6_v2",
-                                 "TY32_W16_S6_v2p"};
-constexpr int kZmCount = 14;
+                                 "TY16_W8_S6_v1", "TY16_W16_S6_v1"};
+constexpr int kZmCount = 9;
 
 int zmarch_configs(const char** names, int max) {
     for (int i = 0; i < kZmCount && names != nullptr && i < max; ++i) names[i] = kZmNames[i];
@@ -852,11 +669,6 @@ static cudaError_t zmarch_cfg(const Launch& L) {
         case 5: return zmarch_t<T, PER, 16, 8, 6, false>(L);
         case 6: return zmarch_t<T, PER, 16, 16, 6, false>(L);
         case 7: return zmarch_t<T, PER, 16, 8, 6, true, 1>(L);
-        case 9: return zmarch_t<T, PER, 16, 16, 6, false, 2>(L);
-        case 10: return zmarch_t<T, PER, 16, 16, 6, true, 2>(L);
-        case 11: return zmarch_t<T, PER, 32, 16, 6, false, 2>(L);
-        case 12: return zmarch_t<T, PER, 16, 8, 6, false, 2>(L);
-        case 13: return zmarch_t<T, PER, 32, 16, 6, true, 2>(L);
         default: return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
     }
 }
