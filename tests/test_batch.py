@@ -74,3 +74,34 @@ def test_graph_replay_and_plain_steppers_agree():
         s.step(p.steps)
         s.synchronize()
         assert np.array_equal(got, s.get())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg", [0, 3])
+def test_long_plan_searches_global_tables(cfg):
+    """A plan whose lookup tables exceed the kernel's shared-memory copy (7000 steps: 56 KB of
+    round offsets) takes the global-memory search path; results stay bit-exact. Run with the
+    default tile configuration and the one that loads two planes ahead."""
+    from pyheat3d_b200 import _lib, heat_stencil, tune
+    from pyheat3d_b200.batch import Batch, Problem
+
+    rng = np.random.default_rng(21)
+    probs = [Problem(rng.random((5, 6, 7), dtype=np.float32), heat_stencil(3, 0.1, "periodic"),
+                     7000, "float32"),
+             Problem(rng.random((9, 40), dtype=np.float32), heat_stencil(2, 0.2, "dirichlet"),
+                     3001, "bfloat16"),
+             Problem(rng.random((6, 17, 33), dtype=np.float32), heat_stencil(3, 0.15, "dirichlet"),
+                     57, "float32")]
+    L = _lib.lib()
+    prev = tune.active_table()
+    tune.use(None)
+    try:
+        _lib.check(L.ph3_tune_set(_lib.KERNEL["batch"], 3, 0, 1, cfg, 0))
+        batch = Batch(probs)
+        batch.run()
+        outs = batch.results()
+    finally:
+        L.ph3_tune_set(_lib.KERNEL["batch"], 3, 0, 1, -1, 0)
+        tune.use(prev)
+    for i, (p, got) in enumerate(zip(probs, outs)):
+        assert np.array_equal(got, _oracle(p)), (i, p.u0.shape, p.steps)
