@@ -60,21 +60,17 @@ constexpr int kW = 8;  // warps per block
 // Compiled tile configurations (the tuning table's batch family): rows per warp and planes per
 // 3D tile, rows per iteration and rows per 2D tile. The plan records which one it was built for.
 template <int CFG> struct BCfg;
-// PD: planes the 3D tiles load ahead.
-template <> struct BCfg<0> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128, PD = 1; };
-template <> struct BCfg<1> { static constexpr int R = 2, ZCH = 16, RB2 = 4, YCH = 64, PD = 1; };
-template <> struct BCfg<2> { static constexpr int R = 8, ZCH = 64, RB2 = 8, YCH = 256, PD = 1; };
-template <> struct BCfg<3> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128, PD = 2; };
-constexpr int kBatchCfgs = 4;
-const char* kBatchNames[kBatchCfgs] = {"R4_Z32_Y128", "R2_Z16_Y64", "R8_Z64_Y256",
-                                       "R4_Z32_Y128_PD2"};
+template <> struct BCfg<0> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128; };
+template <> struct BCfg<1> { static constexpr int R = 2, ZCH = 16, RB2 = 4, YCH = 64; };
+template <> struct BCfg<2> { static constexpr int R = 8, ZCH = 64, RB2 = 8, YCH = 256; };
+constexpr int kBatchCfgs = 3;
+const char* kBatchNames[kBatchCfgs] = {"R4_Z32_Y128", "R2_Z16_Y64", "R8_Z64_Y256"};
 
 struct Geo { int R, ZCH, YCH; };
 Geo geo_of(int cfg) {
     switch (cfg) {
         case 1: return {BCfg<1>::R, BCfg<1>::ZCH, BCfg<1>::YCH};
         case 2: return {BCfg<2>::R, BCfg<2>::ZCH, BCfg<2>::YCH};
-        case 3: return {BCfg<3>::R, BCfg<3>::ZCH, BCfg<3>::YCH};
         default: return {BCfg<0>::R, BCfg<0>::ZCH, BCfg<0>::YCH};
     }
 }
@@ -96,7 +92,7 @@ __device__ __noinline__ void run_tile(const BatchDesc& d, int s, int t) {
     if (d.dims == 3) {
         const int tx = t % d.ntx, ty = (t / d.ntx) % d.nty, tz = t / (d.ntx * d.nty);
         const int z0 = tz * C::ZCH;
-        lite3d_item<T, PER, C::R, true, C::PD>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1, tx,
+        lite3d_item<T, PER, C::R, true>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1, tx,
                                         (ty * kW + w) * C::R, z0, min(z0 + C::ZCH, d.nz));
     } else {
         const int tx = t % d.ntx, ty = t / d.ntx;
@@ -128,16 +124,10 @@ __device__ __forceinline__ long long upper_bound_i64(const long long* a, int n, 
     return lo;
 }
 
-// Shared memory for the block's copy of the plan's lookup tables (round offsets, tile prefix,
-// problem order): with them the dequeue's two binary searches cost shared-memory, not
-// dependent L2, latency. Plans whose tables do not fit search global memory instead.
-constexpr int kTabBytes = 48 * 1024;
-
 __global__ void __launch_bounds__(kThreads, 3)
 batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
     __shared__ int s_p, s_s, s_t;
     __shared__ long long s_item;
-    extern __shared__ __align__(16) long long s_tab[];
     unsigned long long* next = reinterpret_cast<unsigned long long*>(ws);
     int* abort_flag = reinterpret_cast<int*>(ws + 8);
     int* done = reinterpret_cast<int*>(ws + 16);
@@ -151,30 +141,12 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
     const int max_steps = hd->max_steps;
     const int cfg = hd->cfg;
 
-    const long long nr = max_steps + 1, nt = n + 1;
-    if ((nr + nt) * 8 + 4LL * n <= kTabBytes) {
-        long long* r = s_tab;
-        long long* t = s_tab + nr;
-        int* o = reinterpret_cast<int*>(s_tab + nr + nt);
-        for (long long i = threadIdx.x; i < nr; i += blockDim.x) r[i] = round_off[i];
-        for (long long i = threadIdx.x; i < nt; i += blockDim.x) t[i] = tilepre[i];
-        for (int i = threadIdx.x; i < n; i += blockDim.x) o[i] = order[i];
-        __syncthreads();
-        round_off = r;
-        tilepre = t;
-        order = o;
-    }
-
-    // thread 0 fetches the next item number one item ahead, so the atomic's round trip
-    // overlaps the current tile
-    long long nxt = threadIdx.x == 0 ? static_cast<long long>(atomicAdd(next, 1ULL)) : 0;
     for (;;) {
         if (threadIdx.x == 0) {
-            long long item = nxt;
+            long long item = static_cast<long long>(atomicAdd(next, 1ULL));
             if (item >= total || *reinterpret_cast<volatile int*>(abort_flag) != 0) {
                 item = -1;
             } else {
-                nxt = static_cast<long long>(atomicAdd(next, 1ULL));
                 const int s = int(upper_bound_i64(round_off, max_steps + 1, item)) - 1;
                 const long long j = item - round_off[s];
                 const int q = int(upper_bound_i64(tilepre, n + 1, j)) - 1;
@@ -182,8 +154,7 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
                 s_p = p;
                 s_s = s;
                 s_t = int(j - tilepre[q]);
-                // the problem's tiles per step (its tile-prefix increment)
-                const int need = s * int(tilepre[q + 1] - tilepre[q]);
+                const int need = s * desc[p].ntiles;
                 if (!wait_flag_geq(&done[p], need, kSpinLimit, err, abort_flag)) {
                     atomicExch(abort_flag, 1);
                     item = -1;
@@ -199,7 +170,6 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
         switch (cfg) {
             case 1: run_any<1>(d, s, t); break;
             case 2: run_any<2>(d, s, t); break;
-            case 3: run_any<3>(d, s, t); break;
             default: run_any<0>(d, s, t); break;
         }
         __syncthreads();
@@ -216,9 +186,7 @@ int blocks_per_sm_cached() {
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
     if (nb[dev] == 0) {
         int v = 0;
-        // the table copy plus the static shared variables exceed the 48 KB default
-        cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTabBytes);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, batch_kernel, kThreads, kTabBytes) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, batch_kernel, kThreads, 0) !=
                 cudaSuccess ||
             v < 1)
             v = 1;
@@ -433,7 +401,7 @@ cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(ws, 0, counter_bytes(n), stream);
     if (e != cudaSuccess) return e;
     const int grid = sm_count() * blocks_per_sm_cached();
-    batch_kernel<<<grid, kThreads, kTabBytes, stream>>>(static_cast<unsigned char*>(ws), n, err);
+    batch_kernel<<<grid, kThreads, 0, stream>>>(static_cast<unsigned char*>(ws), n, err);
     return cudaGetLastError();
 }
 

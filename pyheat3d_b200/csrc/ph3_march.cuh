@@ -431,7 +431,7 @@ __device__ __forceinline__ void march3d_item(const T* __restrict__ u, T* __restr
 // x-neighbours by shuffles (lane 0 / 31 hold the strip's halo column in one register per row)
 // and, in 3D, loads the rows just above and below its own rows directly.
 // ------------------------------------------------------------------------------------------
-template <typename T, bool PER, int R, bool CG, int PD = 1>
+template <typename T, bool PER, int R, bool CG>
 __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restrict__ o,
                                             const float* __restrict__ b, int nz, int ny, int nx,
                                             float c0, float c1, int strip, int row0, int zlo,
@@ -479,8 +479,15 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
 #pragma unroll
         for (int r = 0; r < R; ++r) bel[r] = ldx1<CG>(pl + roff[r] + cx);
     }
-    auto step = [&](int z, const Plane& ctr, const Plane& abv, Plane& fut) -> bool {
-        if (z + 1 + PD <= zhi) load(z + 1 + PD, fut);
+    // Three planes in turn (centre, above, in flight): the loop runs three planes per pass
+    // and the roles rotate by name, so a loaded plane is never copied and a plane step never
+    // waits for the load it issued.
+    Plane A, B, C;
+    load(zlo, A);
+    load(zlo + 1, B);
+    auto step = [&](int z, const Plane& ctr, const Plane& abv, Plane& pre) -> bool {
+        const bool more = z + 1 < zhi;
+        if (more) load(z + 2, pre);
         T* opl = o + int64_t(z) * P;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -497,28 +504,12 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) bel[r] = ctr.v[r];
-        return z + 1 < zhi;
+        return more;
     };
-    // The planes rotate through 2 + PD registers sets by name (the loop runs 2 + PD planes per
-    // pass), so a loaded plane is never copied and each load has PD plane steps to land.
-    Plane A, B, C;
-    load(zlo, A);
-    load(zlo + 1, B);
-    if constexpr (PD == 1) {
-        for (int z = zlo;;) {
-            if (!step(z++, A, B, C)) break;
-            if (!step(z++, B, C, A)) break;
-            if (!step(z++, C, A, B)) break;
-        }
-    } else {
-        Plane D;
-        if (zlo + 2 <= zhi) load(zlo + 2, C);
-        for (int z = zlo;;) {
-            if (!step(z++, A, B, D)) break;
-            if (!step(z++, B, C, A)) break;
-            if (!step(z++, C, D, B)) break;
-            if (!step(z++, D, A, C)) break;
-        }
+    for (int z = zlo;;) {
+        if (!step(z++, A, B, C)) break;
+        if (!step(z++, B, C, A)) break;
+        if (!step(z++, C, A, B)) break;
     }
 }
 

@@ -317,14 +317,14 @@ tb2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict_
     }
 }
 
-template <typename T, bool PER, int R, int W, int PD>
+template <typename T, bool PER, int R, int W>
 __global__ void __launch_bounds__(32 * W)
 lite3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
               int ny, int nx, float c0, float c1, int zch) {
     const int w = threadIdx.x >> 5;
     const int z0 = blockIdx.z * zch;
-    lite3d_item<T, PER, R, false, PD>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x,
-                                      (blockIdx.y * W + w) * R, z0, min(z0 + zch, nz));
+    lite3d_item<T, PER, R, false>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x,
+                                  (blockIdx.y * W + w) * R, z0, min(z0 + zch, nz));
 }
 
 template <typename T, bool PER, int RB, int W>
@@ -385,7 +385,7 @@ static cudaError_t march_k1_t(const Launch& L) {
     // vector march on unaligned grids); in 2D the raw-row march with 8 rows per step (16384^2:
     // fp32 805 vs 674 GLUPS for the float-window march, bf16 1257 vs 547)
     const int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : 3);
-    if (cfg == 0 || (L.dims == 3 && cfg == 2)) {
+    if (cfg == 0) {
         if (L.dims == 2) {
             constexpr int W = 4, RB = 4;
             const int strips = cdiv(L.nx, 32);
@@ -401,12 +401,8 @@ static cudaError_t march_k1_t(const Launch& L) {
             const int zch = L.chunk > 0 ? L.chunk : default_chunk(L.nz, tiles, 16, 2 * target);
             dim3 grd(cdiv(L.nx, 32), cdiv(L.ny, W * R), cdiv(L.nz, zch));
             if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
-            if (cfg == 2)  // loads two planes ahead
-                lite3d_kernel<T, PER, R, W, 2><<<grd, 32 * W, 0, L.stream>>>(
-                    u, o, L.src, L.nz, L.ny, L.nx, L.c0, L.c1, zch);
-            else
-                lite3d_kernel<T, PER, R, W, 1><<<grd, 32 * W, 0, L.stream>>>(
-                    u, o, L.src, L.nz, L.ny, L.nx, L.c0, L.c1, zch);
+            lite3d_kernel<T, PER, R, W><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.nz, L.ny,
+                                                                     L.nx, L.c0, L.c1, zch);
         }
         return cudaGetLastError();
     }
@@ -523,11 +519,11 @@ cudaError_t launch_tb(const Launch& L) {
 
 // 2D: 0 lean one-column-per-lane march, 1 float-window vector march, 2 / 3 raw-row vector march
 // with 4 / 8 rows per step (shapes without whole 16-byte rows fall back to 1). 3D: 0 lean, 1
-// vector march, 2 lean with loads two planes ahead.
+// vector march.
 int march_configs(int dims, const char** names, int max) {
     static const char* k2[] = {"lane1_W4_RB4", "V16B_W4_RB4", "raw16B_W4_RB4", "raw16B_W4_RB8"};
-    static const char* k3[] = {"lane1_R4_W4", "V16B_R2_W8", "lane1_R4_W4_PD2"};
-    const int n = dims == 2 ? 4 : 3;
+    static const char* k3[] = {"lane1_R4_W4", "V16B_R2_W8"};
+    const int n = dims == 2 ? 4 : 2;
     for (int i = 0; i < n && names != nullptr && i < max; ++i) names[i] = dims == 2 ? k2[i] : k3[i];
     return n;
 }

@@ -77,11 +77,10 @@ def test_graph_replay_and_plain_steppers_agree():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("cfg", [0, 3])
-def test_long_plan_searches_global_tables(cfg):
-    """A plan whose lookup tables exceed the kernel's shared-memory copy (7000 steps: 56 KB of
-    round offsets) takes the global-memory search path; results stay bit-exact. Run with the
-    default tile configuration and the one that loads two planes ahead."""
+@pytest.mark.parametrize("cfg", [0, 1])
+def test_long_plan_with_few_tiles_per_step(cfg):
+    """Long dependency chains (7000 and 3001 steps of grids that are one or two tiles each)
+    beside a short problem stay bit-exact, for two tile configurations."""
     from pyheat3d_b200 import _lib, heat_stencil, tune
     from pyheat3d_b200.batch import Batch, Problem
 
