@@ -370,6 +370,16 @@ def run_b200(a: argparse.Namespace) -> None:
             except Exception as e:  # pragma: no cover
                 variants["2d16384_" + key.split("/")[1]] = {"error": str(e)[:200]}
         del u2
+        # the largest configured grid: 3D 1024^3 fp32, 4 GiB per field
+        u3 = field(2 * N3, 3)
+        for key in ("b200/zmarch", "b200/tb4"):
+            try:
+                variants["3d1024_" + key.split("/")[1]] = variant_row(torch, key, u3, stencil,
+                                                                      min(T, 200), copy_bw)
+            except Exception as e:  # pragma: no cover
+                variants["3d1024_" + key.split("/")[1]] = {"error": str(e)[:200]}
+        del u3
+        torch.cuda.empty_cache()
 
     # ---- CPU baseline (rank 0, N = 1)
     cpu = None
