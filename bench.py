@@ -89,6 +89,18 @@ def peaks() -> tuple[float, str]:
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def workload_config(dims: int, n: int, storage: str, tsteps: int, ws: int) -> dict:
+    """The `config` object of both arms' JSON lines (the same workload; `time_steps_per_step`
+    is the part of a solve one bench step covers)."""
+    return {"workload": f"{dims}D {n}^{dims} {storage} periodic heat, r=0.95/{2 * dims}, "
+                        "uniform[0,1) fields, seed 0 (rank r: seed r)",
+            "grid": [n] * dims, "bc": "periodic", "storage": storage,
+            "time_steps_per_step": tsteps, "units": "site updates (all cells)",
+            "l2": f"inputs larger than L2 ({n ** dims * (4 if storage == 'float32' else 2) >> 20}"
+                  " MiB field vs 126 MB L2)",
+            "parallelism": f"replicas x{ws}"}
+
+
 def field(n: int, dims: int, seed: int = 0) -> np.ndarray:
     return np.random.default_rng(seed).random((n,) * dims, dtype=np.float32)
 
@@ -419,13 +431,7 @@ def run_b200(a: argparse.Namespace) -> None:
             "value": round(value, 2), "kernel": a.variant, "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": round(secs / K * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{a.dims}D {a.n}^{a.dims} {var.storage} periodic heat, "
-                                   f"r=0.95/{2 * a.dims}, "
-                                   f"uniform[0,1) seed 0 (rank r: seed r), {a.variant}",
-                       "grid": [a.n] * a.dims, "bc": "periodic", "storage": var.storage,
-                       "time_steps_per_step": T, "units": "site updates (all cells)",
-                       "l2": "inputs larger than L2 (512 MiB field vs 126 MB L2)",
-                       "parallelism": f"replicas x{ws}"},
+            "config": workload_config(a.dims, a.n, var.storage, T, ws),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
                          "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                          "traffic": traffic, "peak_kind": peak_kind,
@@ -599,9 +605,7 @@ def run_reference(a: argparse.Namespace) -> None:
         "value": round(value, 4), "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
         "ms_per_step": round(secs / K * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "3D 512^3 fp32 periodic heat, r=0.95/6, uniform[0,1) seed 0",
-                   "grid": [N3, N3, N3], "bc": "periodic", "storage": "float32",
-                   "time_steps_per_step": sweeps, "units": "site updates (all cells)"},
+        "config": workload_config(3, N3, "float32", sweeps, ws),
         "cpu_baseline": {"value": round(value, 4), "unit": "GLUPS", "cores": cores,
                          "kind": "port",
                          "sample": f"{sweeps} update of the 512^3 field per step, NumPy oracle "
