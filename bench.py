@@ -456,10 +456,10 @@ def run_b200(a: argparse.Namespace) -> None:
 
 
 # ---------------------------------------------------------------------------------------------
-# configs 3-5: precision, batching, serving (1-GPU runs; reported beside the headline)
+# precision, batching and serving workloads (1-GPU runs; reported beside the headline)
 # ---------------------------------------------------------------------------------------------
 def bench_batching(torch) -> dict:
-    """512 uneven grids (config 4): one persistent launch in a CUDA graph vs per-grid launches."""
+    """512 uneven grids: one persistent launch in a CUDA graph vs per-grid launches."""
     import ctypes
 
     from oracle import run_reference
@@ -525,7 +525,7 @@ def bench_batching(torch) -> dict:
 
 
 def bench_serving(torch, seconds: float) -> dict:
-    """Poisson stream, 2000 req/s (config 5): continuous batching vs one solve at a time."""
+    """Poisson stream, 2000 req/s: continuous batching vs one solve at a time."""
     from pyheat3d_b200.serve import GpuExecutor, PlainServer, Server, poisson_stream
 
     reqs = poisson_stream(2000.0, seconds, seed=0)
@@ -545,7 +545,7 @@ def bench_serving(torch, seconds: float) -> dict:
 
 
 def bench_precision(torch, n: int = 256) -> dict:
-    """3D Poisson 256^3 by FP64 defect correction around 16-bit Jacobi (config 3)."""
+    """3D Poisson 256^3 by FP64 defect correction around 16-bit Jacobi."""
     from oracle.precision import discrete_solution, manufactured
     from pyheat3d_b200.precision import DefectCorrection
 

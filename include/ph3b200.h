@@ -32,7 +32,7 @@ extern "C" {
 #define PH3_OK 0
 #define PH3_EINVAL 1       /* invalid argument (shape, pointer, storage, k, ...) */
 #define PH3_ECUDA 2        /* a CUDA runtime call failed (message has the CUDA error string) */
-#define PH3_EUNSUPPORTED 3 /* valid request this build cannot serve (e.g. grid too large) */
+#define PH3_EUNSUPPORTED 3 /* valid request this library cannot serve (e.g. grid too large) */
 #define PH3_EDEVICE 4      /* a kernel reported an expired bounded wait (see ph3_device_status) */
 
 /* storage types (stencil.cu:16-30 STORAGE macro: 0 fp32, 1 fp16, 2 bf16) */

@@ -2,8 +2,8 @@
 
 When pyheat3d is importable its own classes are used, so a ``B200Stepper`` *is* a
 ``pyheat3d.backends.base.Stepper`` and the variants enter ``pyheat3d.registry.VARIANTS``
-unchanged. Without pyheat3d (e.g. on a bare GPU box) this module provides same-named mirrors with
-the same fields, argument meaning and errors:
+unchanged. Without pyheat3d (on a machine where only this package is installed) this module
+provides same-named mirrors with the same fields, argument meaning and errors:
 
 - ``Stencil``, ``heat_stencil``, ``jacobi_stencil``, ``stability_limit``:
   pyheat3d ``src/pyheat3d/problem.py:33-69``

@@ -14,7 +14,7 @@ vectors come from ``validation.round_storage``) and the problem constructors
   (storage, k) rounding schedules, 197 steps (every k of 2, 3, 4, 8 plus a remainder, as in the
   reference's ``tests/test_backends.py:40``), plus Jacobi sweeps with and without a source,
   float64 runs and the tiny-grid cases of ``tests/test_backends.py:86-103``;
-- ``config1.json``: SHA-256 and summary statistics of the 3D 128^3 Dirichlet heat run
+- ``dirichlet128.json``: SHA-256 and summary statistics of the 3D 128^3 Dirichlet heat run
   (r = 0.15, seed 0, zero boundary layer, 100 steps), too large to store as an array.
 """
 
@@ -91,7 +91,7 @@ def main() -> None:
         arrays["round_f16"] = val.round_storage(special, "float16")
     np.savez_compressed(HERE / "stencil_small.npz", **arrays)
 
-    # config 1: 128^3 fp32 Dirichlet, zero walls, r = 0.15, seed 0, 100 steps
+    # the 128^3 fp32 Dirichlet case: zero walls, r = 0.15, seed 0, 100 steps
     u0 = np.random.default_rng(0).random((128,) * 3, dtype=np.float32)
     u0[0] = u0[-1] = 0
     u0[:, 0] = u0[:, -1] = 0
@@ -100,15 +100,15 @@ def main() -> None:
     s = NumpyStepper(u0, st)
     s.step(100)
     u = s.get()
-    meta["config1"] = {
+    meta["dirichlet128"] = {
         "shape": [128, 128, 128], "r": 0.15, "steps": 100, "seed": 0, "bc": "dirichlet",
         "c0": st.c0, "c1": st.c1,
         "sha256": hashlib.sha256(np.ascontiguousarray(u).tobytes()).hexdigest(),
         "sum64": float(u.astype(np.float64).sum()), "max": float(u.max()),
         "probe": [float(u[64, 64, 64]), float(u[1, 1, 1]), float(u[100, 7, 33])],
     }
-    (HERE / "config1.json").write_text(json.dumps(meta, indent=1, default=list))
-    print("wrote", HERE / "stencil_small.npz", "and", HERE / "config1.json")
+    (HERE / "dirichlet128.json").write_text(json.dumps(meta, indent=1, default=list))
+    print("wrote", HERE / "stencil_small.npz", "and", HERE / "dirichlet128.json")
 
 
 if __name__ == "__main__":

@@ -26,7 +26,7 @@ from oracle import (
 
 GOLD = Path(__file__).resolve().parent / "golden"
 G = np.load(GOLD / "stencil_small.npz")
-META = json.loads((GOLD / "config1.json").read_text())
+META = json.loads((GOLD / "dirichlet128.json").read_text())
 STEPS = META["steps"]
 SCHEDULES = [tuple(x) for x in META["schedules"]]
 
@@ -117,9 +117,9 @@ def test_threaded_step_is_bitwise_reference_step(dims, bc, src, dtype):
     assert np.array_equal(out, ref)
 
 
-def test_config1_hash_matches_reference_run():
+def test_dirichlet128_hash_matches_reference_run():
     """3D 128^3 Dirichlet, zero walls, r = 0.15, seed 0, 100 steps: SHA-256 of the result."""
-    cfg = META["config1"]
+    cfg = META["dirichlet128"]
     u0 = np.random.default_rng(0).random((128,) * 3, dtype=np.float32)
     u0[0] = u0[-1] = 0
     u0[:, 0] = u0[:, -1] = 0

@@ -141,9 +141,9 @@ def test_small_grids_smaller_than_one_tile():
                     _assert_same(_run(key, u0, st, 9), _ref(key, u0, st, 9), (key, bc))
 
 
-def test_config1_128_cubed_dirichlet_matches_reference_hash():
+def test_dirichlet_128_cubed_matches_reference_hash():
     """3D 128^3 fp32, zero walls, r = 0.15, seed 0, 100 steps: SHA-256 of the reference result."""
-    cfg = json.loads((GOLD / "config1.json").read_text())["config1"]
+    cfg = json.loads((GOLD / "dirichlet128.json").read_text())["dirichlet128"]
     u0 = np.random.default_rng(0).random((128,) * 3, dtype=np.float32)
     u0[0] = u0[-1] = 0
     u0[:, 0] = u0[:, -1] = 0
