@@ -13,10 +13,13 @@ z-march kernel (``b200/zmarch``). One bench *step* is one solve of ``--time-step
 - ``roofline``: the z-march kernel's algorithmic bytes (8 B per fp32 update: one read and one
   write of every value) per launch over its average launch time, against the measured HBM copy
   bandwidth.
-- ``variants``: the other kernels of the same workload (tb2/3/4/8, 16-bit storage) and the 2D
-  16384^2 fp32 periodic grid (r = 0.95/4), one solve each, for the per-variant roofline figures.
+- ``variants``: the other kernels of the same workload (naive, tb2/3/4/8, 16-bit storage), the 2D
+  16384^2 fp32 periodic grid (r = 0.95/4) and the 3D 1024^3 fp32 grid (4 GiB per field), one
+  solve each, for the per-variant roofline figures.
 - ``cpu_baseline``: the NumPy oracle (pyheat3d's reference algorithm restated) on this host, on a
   bounded sample of the same workload.
+- ``precision``, ``batching``, ``serving``: the defect-correction solve of the 256^3 Poisson
+  problem, the 512-grid batch and the 2000 req/s request stream (``--no-…`` flags skip them).
 
 ``--impl reference`` times the reference's CPU path (the NumPy oracle, thread-chunked over
 z-slabs with every host core) on the same workload and prints the same line with
