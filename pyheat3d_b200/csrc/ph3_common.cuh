@@ -207,7 +207,23 @@ __device__ __forceinline__ float2 upd2_x2(float2 c0, float2 c1, float2 ctr, floa
     return lin2(c0, c1, ctr, s);
 }
 
+// Periodic index in [0, n).
 __device__ __forceinline__ int wrap_idx(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+// The same result for every i, with compare-and-add paths for indices within one period of the
+// domain (halos and tile overhangs) so only far indices pay for a division. Faster where an
+// index is wrapped once per plane or row of the temporal-blocking kernels; the division-free
+// branches are not used in the register marches, whose unrolled row loads they would separate
+// (measured: the 2D raw-row march at half speed with them).
+__device__ __forceinline__ int wrap_near(int i, int n) {
+    if (i >= 0) {
+        if (i < n) return i;
+        if (i - n < n) return i - n;
+    } else if (i >= -n) {
+        return i + n;
+    }
     i %= n;
     return i < 0 ? i + n : i;
 }

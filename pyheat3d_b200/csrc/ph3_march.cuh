@@ -44,6 +44,11 @@ __device__ __forceinline__ int fix_idx(int i, int n) {
     if constexpr (PER) return wrap_idx(i, n);
     else return clamp_idx(i, 0, n - 1);
 }
+template <bool PER>
+__device__ __forceinline__ int fix_near(int i, int n) {  // fix_idx through wrap_near
+    if constexpr (PER) return wrap_near(i, n);
+    else return clamp_idx(i, 0, n - 1);
+}
 
 // Column addressing of one thread's V consecutive x-values starting at gx.
 // vec: the V values are one aligned vector (nx % V == 0 and gx % V == 0), addressed by `base`.

@@ -121,7 +121,7 @@ tb3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict_
     cols.init(gx, nx, vec);
     int64_t roff[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) roff[r] = int64_t(fix_idx<PER>(gy0 + r, ny)) * nx;
+    for (int r = 0; r < R; ++r) roff[r] = int64_t(fix_near<PER>(gy0 + r, ny)) * nx;
     uint32_t fixx = 0, fixy = 0;  // Dirichlet: boundary or outside sites keep their value
     if constexpr (!PER) {
 #pragma unroll
@@ -146,7 +146,7 @@ tb3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict_
 
     float pre[R][V];
     auto load_plane = [&](int z, float (&dst)[R][V]) {
-        const T* pl = u + int64_t(fix_idx<PER>(z, nz)) * P;
+        const T* pl = u + int64_t(fix_near<PER>(z, nz)) * P;
 #pragma unroll
         for (int r = 0; r < R; ++r) cols.load(pl + roff[r], vec, dst[r]);
     };
@@ -186,7 +186,7 @@ tb3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict_
                 for (int j = 0; j < V; ++j) { up[j] = q[s - 1][1][0][j]; dn[j] = q[s - 1][1][R - 1][j]; }
             }
             const bool zfix = !PER && (c <= 0 || c >= nz - 1);
-            const float* bpl = b != nullptr ? b + int64_t(fix_idx<PER>(c, nz)) * P : nullptr;
+            const float* bpl = b != nullptr ? b + int64_t(fix_near<PER>(c, nz)) * P : nullptr;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const float left = __shfl_up_sync(kFull, q[s - 1][1][r][V - 1], 1);
@@ -271,7 +271,7 @@ tb2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict_
 #pragma unroll
             for (int j = 0; j < V; ++j) q[s][a][j] = 0.f;
     float pre[V];
-    cols.load(u + int64_t(fix_idx<PER>(y0 - K, ny)) * nx, vec, pre);
+    cols.load(u + int64_t(fix_near<PER>(y0 - K, ny)) * nx, vec, pre);
 
     for (int iy = y0 - K; iy < y1 + K; ++iy) {
 #pragma unroll
@@ -280,7 +280,7 @@ tb2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict_
             q[0][1][j] = q[0][2][j];
             q[0][2][j] = pre[j];
         }
-        if (iy + 1 < y1 + K) cols.load(u + int64_t(fix_idx<PER>(iy + 1, ny)) * nx, vec, pre);
+        if (iy + 1 < y1 + K) cols.load(u + int64_t(fix_near<PER>(iy + 1, ny)) * nx, vec, pre);
         float res[V];
 #pragma unroll
         for (int s = 1; s <= K; ++s) {
@@ -289,7 +289,7 @@ tb2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict_
             const float left = __shfl_up_sync(kFull, q[s - 1][1][V - 1], 1);
             const float right = __shfl_down_sync(kFull, q[s - 1][1][0], 1);
             float bv[V];
-            if (b != nullptr) cols.load_src(b + int64_t(fix_idx<PER>(c, ny)) * nx, vec, bv);
+            if (b != nullptr) cols.load_src(b + int64_t(fix_near<PER>(c, ny)) * nx, vec, bv);
 #pragma unroll
             for (int j = 0; j < V; ++j) {
                 const float ctr = q[s - 1][1][j];

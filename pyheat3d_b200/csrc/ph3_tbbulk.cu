@@ -124,26 +124,27 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
     // and copies its own R rows of each plane (lanes 0..R-1, one row each), announcing their
     // bytes on the stage's mbarrier. A stage is refilled one plane after it was consumed: by
     // then every warp has passed the named barriers of that iteration, so all reads are done.
-    int is_item = blockIdx.x, is_iz = 0, is_zend = 0;
+    int is_item = blockIdx.x, is_iz = 0, is_zend = 0, is_xs = 0, is_ys = 0;
     uint32_t is_it = 0;
-    auto cursor_item = [&](int item) {
+    auto cursor_item = [&](int item) {  // the item's tile origin, computed once per item
         if (item >= g.nitems) return;
         const int ch = item / (g.ntx * g.nty);
         const int z0 = ch * g.zch, z1 = min(z0 + g.zch, g.nz);
         is_iz = z0 - K;
         is_zend = z1 + K;
+        is_xs = (item % g.ntx) * OX - KX;
+        is_ys = ((item / g.ntx) % g.nty) * OY - K;
     };
     auto issue_next = [&]() {
         if (is_item >= g.nitems) return;
-        const int tx = is_item % g.ntx, ty = (is_item / g.ntx) % g.nty;
-        const int xs = tx * OX - KX, ys = ty * OY - K;
+        const int xs = is_xs, ys = is_ys;
         const int s = is_it % STAGES;
-        const int pz = PER ? wrap_idx(is_iz, g.nz) : clamp_idx(is_iz, 0, g.nz - 1);
+        const int pz = PER ? wrap_near(is_iz, g.nz) : clamp_idx(is_iz, 0, g.nz - 1);
         if (lane == 0) mbar_arrive_expect_tx(&full[s], R * C::ROW_BYTES);
         __syncwarp();
         T* plane = ring + s * (EY * EX);
         for (int r = warp * R + lane; r < warp * R + R && lane < R; r += 32) {
-            const int gy = PER ? wrap_idx(ys + r, g.ny) : clamp_idx(ys + r, 0, g.ny - 1);
+            const int gy = PER ? wrap_near(ys + r, g.ny) : clamp_idx(ys + r, 0, g.ny - 1);
             const T* row = u + int64_t(pz) * P + int64_t(gy) * g.nx;
             T* dst = plane + r * EX;
             int done = 0;
@@ -151,7 +152,7 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 const int x = xs + done;
                 int src, len;
                 if (PER) {
-                    src = wrap_idx(x, g.nx);
+                    src = wrap_near(x, g.nx);
                     len = min(EX - done, g.nx - src);
                 } else if (x < 0) {  // outside the domain: any in-range data will do
                     src = 0;
@@ -199,7 +200,7 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 if (gy0 + r <= 0 || gy0 + r >= g.ny - 1) fixy |= 1u << r;
         }
         const bool xwriter = lx >= KX && lx < KX + OX && gx < g.nx;
-        const int bcol = PER ? wrap_idx(gx, g.nx) : clamp_idx(gx, 0, g.nx - V);
+        const int bcol = PER ? wrap_near(gx, g.nx) : clamp_idx(gx, 0, g.nx - V);
 #pragma unroll
         for (int s = 0; s < K; ++s)
 #pragma unroll
@@ -251,7 +252,7 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 const bool zfix = !PER && (c <= 0 || c >= g.nz - 1);
                 const float* bpl = nullptr;
                 if (b != nullptr)
-                    bpl = b + int64_t(PER ? wrap_idx(c, g.nz) : clamp_idx(c, 0, g.nz - 1)) * P;
+                    bpl = b + int64_t(PER ? wrap_near(c, g.nz) : clamp_idx(c, 0, g.nz - 1)) * P;
                 float2 res[R][NP];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
@@ -259,7 +260,7 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                     const float right = __shfl_down_sync(kFull, A[lev - 1][r][0].x, 1);
                     float2 bv[NP];
                     if (bpl != nullptr) {
-                        const int gy = PER ? wrap_idx(gy0 + r, g.ny) : clamp_idx(gy0 + r, 0, g.ny - 1);
+                        const int gy = PER ? wrap_near(gy0 + r, g.ny) : clamp_idx(gy0 + r, 0, g.ny - 1);
                         float f[V];
                         ld_vec<float, V>(bpl + int64_t(gy) * g.nx + bcol, f);
 #pragma unroll
