@@ -38,15 +38,23 @@ import numpy as np
 from . import _lib
 
 DEFAULT_TABLE = Path(__file__).resolve().with_name("tuning.json")
-CLASSES = ((1 << 22, "small"), (1 << 26, "medium"), (None, "large"))
+CLASSES = ((1 << 22, "small"), (1 << 26, "medium"), (1 << 29, "large"), (None, "xlarge"))
 
 
 def shape_class(cells: int) -> str:
-    """'small' (< 4 Mi sites), 'medium' (< 64 Mi) or 'large'."""
+    """'small' (< 4 Mi sites), 'medium' (< 64 Mi), 'large' (< 512 Mi, e.g. 512^3) or 'xlarge'
+    (e.g. 1024^3)."""
     for bound, name in CLASSES:
         if bound is None or cells < bound:
             return name
-    return "large"
+    return "xlarge"
+
+
+def _nearest_classes(cls: str) -> list[str]:
+    """`cls` first, then the other classes by distance (the larger one first on a tie)."""
+    names = [name for _, name in CLASSES]
+    i = names.index(cls)
+    return sorted(names, key=lambda c: (abs(names.index(c) - i), -names.index(c)))
 
 
 def _key(kernel: str, dims: int, storage: str, k: int, cls: str) -> str:
@@ -74,16 +82,14 @@ class Table:
         return cls(json.loads(Path(path).read_text()))
 
     def entry(self, kernel: str, dims: int, storage: str, k: int, cells: int) -> dict | None:
-        cls_ = shape_class(cells)
-        for c in (cls_, "large", "medium", "small"):  # nearest available class
+        for c in _nearest_classes(shape_class(cells)):  # nearest available class
             e = self.entries.get(_key(kernel, dims, storage, k, c))
             if e is not None:
                 return e
         return None
 
     def best_for(self, dims: int, storage: str, cells: int) -> dict | None:
-        cls_ = shape_class(cells)
-        for c in (cls_, "large", "medium", "small"):
+        for c in _nearest_classes(shape_class(cells)):
             b = self.best.get(f"{dims}:{storage}:{c}")
             if b is not None:
                 return b

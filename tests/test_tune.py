@@ -13,6 +13,19 @@ def test_shape_classes():
     assert tune.shape_class(64 ** 3) == "small"
     assert tune.shape_class(256 ** 3) == "medium"
     assert tune.shape_class(512 ** 3) == "large"
+    assert tune.shape_class(1024 ** 3) == "xlarge"
+
+
+def test_nearest_class_order():
+    assert tune._nearest_classes("large") == ["large", "xlarge", "medium", "small"]
+    assert tune._nearest_classes("xlarge") == ["xlarge", "large", "medium", "small"]
+    assert tune._nearest_classes("small") == ["small", "medium", "large", "xlarge"]
+    t = tune.Table({})
+    t.entries["tb:3:float32:4:large"] = {"cfg": 0, "chunk": 0, "glups": 1.0}
+    t.entries["tb:3:float32:4:xlarge"] = {"cfg": 1, "chunk": 64, "glups": 1.0}
+    assert t.entry("tb", 3, "float32", 4, 1024 ** 3)["cfg"] == 1
+    assert t.entry("tb", 3, "float32", 4, 512 ** 3)["cfg"] == 0
+    assert t.entry("tb", 3, "float32", 4, 128 ** 3)["cfg"] == 0  # medium: nearest is large
 
 
 def test_table_roundtrip_and_lookup(tmp_path):
