@@ -296,6 +296,24 @@ def pick_best(table: Table, dims: int, storage: str, n: int, ks=(1, 2, 3, 4, 8),
     return rec
 
 
+def report(table: Table) -> str:
+    """Markdown view of a table: the winning configuration per entry and the fastest kernel
+    (single step or tb<k>) per (dims, storage, shape class)."""
+    out = ["| family:dims:storage:k:class | winning config | chunk | GLUPS |", "|---|---|---:|---:|"]
+    for key in sorted(table.entries):
+        e = table.entries[key]
+        out.append(f"| `{key}` | {e.get('cfg_name', e.get('cfg'))} | {e.get('chunk', 0)} | "
+                   f"{e.get('glups', '')} |")
+    out += ["", "| dims:storage:class | k=1 | k=2 | k=3 | k=4 | k=8 | chosen |",
+            "|---|---:|---:|---:|---:|---:|---|"]
+    for key in sorted(table.best):
+        b = table.best[key]
+        cells = " | ".join(str(b.get("all", {}).get(str(k), "-")) for k in (1, 2, 3, 4, 8))
+        chosen = "single step" if b["k"] == 1 else f"tb k={b['k']}"
+        out.append(f"| `{key}` (n={b.get('n')}) | {cells} | {chosen} |")
+    return "\n".join(out)
+
+
 # ------------------------------------------------------------------------------------------
 # CLI
 # ------------------------------------------------------------------------------------------
@@ -303,7 +321,7 @@ def main(argv: list[str] | None = None) -> int:
     ap = argparse.ArgumentParser(description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("what", choices=("b200-zmarch", "b200-ymarch", "b200-tb3d", "b200-tb2d",
-                                     "b200-batch", "all"))
+                                     "b200-batch", "all", "report"))
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--K", type=int, nargs="*", default=None)
     ap.add_argument("--storage", nargs="*", default=["float32", "bfloat16"])
@@ -312,6 +330,10 @@ def main(argv: list[str] | None = None) -> int:
     ap.add_argument("--out", default=None, help="table to update (default: the active table "
                                                 "path, pyheat3d_b200/tuning.json)")
     a = ap.parse_args(argv)
+    if a.what == "report":  # the table as Markdown (no GPU needed)
+        path = Path(a.out or os.environ.get("PH3_TUNING") or DEFAULT_TABLE)
+        print(report(Table.load(path)))
+        return 0
     import torch
 
     if not torch.cuda.is_available():

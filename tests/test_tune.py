@@ -83,3 +83,14 @@ def test_module_entry_point_runs_the_package_module(monkeypatch):
     with pytest.raises(SystemExit) as e:
         runpy.run_module("pyheat3d_b200.tune", run_name="__main__")
     assert e.value.code == 0 and called == [None]
+
+
+def test_report_lists_entries_and_choices():
+    t = tune.Table({})
+    t.entries["tb:3:float32:4:xlarge"] = {"cfg": 0, "cfg_name": "V4_R2_W16_S4", "chunk": 0,
+                                          "glups": 782.5}
+    t.best["3:float32:xlarge"] = {"k": 4, "variant": "tb", "glups": 782.5, "n": 1024,
+                                  "all": {"1": 717.4, "4": 782.5}}
+    md = tune.report(t)
+    assert "| `tb:3:float32:4:xlarge` | V4_R2_W16_S4 | 0 | 782.5 |" in md
+    assert "| `3:float32:xlarge` (n=1024) | 717.4 | - | - | 782.5 | - | tb k=4 |" in md
