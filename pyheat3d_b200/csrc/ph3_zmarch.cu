@@ -346,8 +346,9 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
     }
 }
 
-// First form of the consumer (scalar float registers, modulo stage indexing, no register cap):
-// kept as a selectable configuration because it is measured beside the packed form.
+// First form of the consumer (scalar float registers, no register cap): kept as a selectable
+// configuration because it is measured beside the packed form. The ring stage and parity of
+// the next plane advance incrementally (no division by the stage count per plane).
 template <typename T, bool PER, int TY, int NWC, int STAGES>
 __global__ void __launch_bounds__(32 * (NWC + 1))
 zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
@@ -383,7 +384,13 @@ zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
 
     // --------------------------------------------------------------------- consumer warps
     const int r0 = warp * RW;  // first tile row of this warp
-    uint32_t it = 0;
+    uint32_t it = 0;           // planes taken
+    int st = 0;                // ring stage of plane `it` (it % STAGES, kept incrementally)
+    uint32_t ph = 0;           // its full-barrier parity ((it / STAGES) & 1)
+    auto advance = [&]() {
+        ++it;
+        if (++st == STAGES) { st = 0; ph ^= 1u; }
+    };
     bool ok = true;
     auto body_row = [&](int s, int row) -> const T* {
         return reinterpret_cast<const T*>(smem + s * C::STAGE_BYTES) + row * TX;
@@ -433,22 +440,28 @@ zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
 
         // plane zlo-1: only the own values are needed
         {
-            const int s = it % STAGES;
-            if (!mbar_wait(&full[s], (it / STAGES) & 1u, err)) { ok = false; break; }
+            const int s = st;
+            if (!mbar_wait(&full[s], ph, err)) { ok = false; break; }
 #pragma unroll
             for (int r = 0; r < RW; ++r) lds_vec(body_row(s, r0 + r + 1) + lane * V, bel[r]);
             release(s);
-            ++it;
+            advance();
         }
-        int sc = it % STAGES;  // stage of the centre plane
-        if (!mbar_wait(&full[sc], (it / STAGES) & 1u, err)) { ok = false; break; }
+        int sc = st;  // stage of the centre plane
+        if (!mbar_wait(&full[sc], ph, err)) { ok = false; break; }
 #pragma unroll
         for (int r = 0; r < RW; ++r) lds_vec(body_row(sc, r0 + r + 1) + lane * V, ctr[r]);
-        ++it;
+        advance();
+        // periodic partial tile: the row after ny-1 is the halo row loaded from row 0
+        int wrap_r = -1;
+        if (PER && y0 + TY > g.ny) {
+            const int rr = g.ny - 1 - (y0 + r0);
+            if (rr >= 0 && rr < RW) wrap_r = rr;
+        }
 
         for (int z = zlo; z < zhi; ++z) {
-            const int sa = it % STAGES;
-            if (!mbar_wait(&full[sa], (it / STAGES) & 1u, err)) { ok = false; break; }
+            const int sa = st;
+            if (!mbar_wait(&full[sa], ph, err)) { ok = false; break; }
 #pragma unroll
             for (int r = 0; r < RW; ++r) lds_vec(body_row(sa, r0 + r + 1) + lane * V, abv[r]);
             SrcRows<RW, V> bcur;
@@ -457,12 +470,6 @@ zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
                 if (z + 1 < zhi) bnext.load(b, int64_t(z + 1) * P, boff);
             }
             // y-neighbours of the first and last rows come from the staged centre plane
-            // periodic partial tile: the row after ny-1 is the halo row loaded from row 0
-            int wrap_r = -1;
-            if (PER && y0 + TY > g.ny) {
-                const int rr = g.ny - 1 - (y0 + r0);
-                if (rr >= 0 && rr < RW) wrap_r = rr;
-            }
             float up[V], dn[V], wdn[V];
             lds_vec(body_row(sc, r0) + lane * V, up);
             lds_vec(body_row(sc, wrap_r == RW - 1 ? TY + 1 : r0 + RW + 1) + lane * V, dn);
@@ -518,7 +525,7 @@ zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
                     ctr[r][j] = abv[r][j];
                 }
             sc = sa;
-            ++it;
+            advance();
         }
         if (!ok) break;
         release(sc);  // plane zhi
