@@ -269,11 +269,14 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
                         const float2 ctr = A[lev - 1][r][p];
-                        const float2 xm = make_float2(p > 0 ? A[lev - 1][r][p - 1].y : left, ctr.x);
-                        const float2 xp = make_float2(ctr.y, p < NP - 1 ? A[lev - 1][r][p + 1].x : right);
+                        // x-neighbour sums by scalar adds straight into a register pair (no
+                        // pairs of misaligned neighbours to assemble)
+                        const float xl = p > 0 ? A[lev - 1][r][p - 1].y : left;
+                        const float xr = p < NP - 1 ? A[lev - 1][r][p + 1].x : right;
+                        const float2 sx = make_float2(__fadd_rn(xl, ctr.y), __fadd_rn(ctr.x, xr));
                         const float2 ym = r > 0 ? A[lev - 1][r - 1][p] : up[p];
                         const float2 yp = r < R - 1 ? A[lev - 1][r + 1][p] : dn[p];
-                        float2 v = upd3_x2(c0v, c1v, ctr, xm, xp, ym, yp, B[lev - 1][r][p], N[r][p]);
+                        float2 v = upd3_sx2(c0v, c1v, ctr, sx, ym, yp, B[lev - 1][r][p], N[r][p]);
                         if (bpl != nullptr) v = add2(v, bv[p]);
                         if constexpr (!PER) {
                             const bool fr = zfix || ((fixy >> r) & 1u);
