@@ -208,7 +208,7 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
 #pragma unroll
                 for (int p = 0; p < NP; ++p) A[s][r][p] = B[s][r][p] = make_float2(0.f, 0.f);
 
-        for (int iz = z0 - K; iz < z1 + K; ++iz, ++it) {
+        auto step = [&](int iz, float2 (&Bp)[K][R][NP], float2 (&Ap)[K][R][NP]) {
             if (ok) issue_next();
             const int s = it % STAGES;
             if (ok) {
@@ -232,21 +232,21 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 const int c = iz - lev;
                 // y-neighbours of the first / last row: exchange with the adjacent warps
                 float* eb = edge + buf * (2 * NWC * EX);
-                put_lane<NP>(eb + warp * EX + lx, A[lev - 1][0]);
-                put_lane<NP>(eb + (NWC + warp) * EX + lx, A[lev - 1][R - 1]);
+                put_lane<NP>(eb + warp * EX + lx, Ap[lev - 1][0]);
+                put_lane<NP>(eb + (NWC + warp) * EX + lx, Ap[lev - 1][R - 1]);
                 named_sync(1, NWC * 32);
                 float2 up[NP], dn[NP];
                 if (warp > 0) {
                     get_lane<NP>(eb + (NWC + warp - 1) * EX + lx, up);
                 } else {
 #pragma unroll
-                    for (int p = 0; p < NP; ++p) up[p] = A[lev - 1][0][p];
+                    for (int p = 0; p < NP; ++p) up[p] = Ap[lev - 1][0][p];
                 }
                 if (warp < NWC - 1) {
                     get_lane<NP>(eb + (warp + 1) * EX + lx, dn);
                 } else {
 #pragma unroll
-                    for (int p = 0; p < NP; ++p) dn[p] = A[lev - 1][R - 1][p];
+                    for (int p = 0; p < NP; ++p) dn[p] = Ap[lev - 1][R - 1][p];
                 }
                 buf ^= 1;
                 const bool zfix = !PER && (c <= 0 || c >= g.nz - 1);
@@ -256,8 +256,8 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 float2 res[R][NP];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const float left = __shfl_up_sync(kFull, A[lev - 1][r][NP - 1].y, 1);
-                    const float right = __shfl_down_sync(kFull, A[lev - 1][r][0].x, 1);
+                    const float left = __shfl_up_sync(kFull, Ap[lev - 1][r][NP - 1].y, 1);
+                    const float right = __shfl_down_sync(kFull, Ap[lev - 1][r][0].x, 1);
                     float2 bv[NP];
                     if (bpl != nullptr) {
                         const int gy = PER ? wrap_near(gy0 + r, g.ny) : clamp_idx(gy0 + r, 0, g.ny - 1);
@@ -268,15 +268,15 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                     }
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
-                        const float2 ctr = A[lev - 1][r][p];
+                        const float2 ctr = Ap[lev - 1][r][p];
                         // x-neighbour sums by scalar adds straight into a register pair (no
                         // pairs of misaligned neighbours to assemble)
-                        const float xl = p > 0 ? A[lev - 1][r][p - 1].y : left;
-                        const float xr = p < NP - 1 ? A[lev - 1][r][p + 1].x : right;
+                        const float xl = p > 0 ? Ap[lev - 1][r][p - 1].y : left;
+                        const float xr = p < NP - 1 ? Ap[lev - 1][r][p + 1].x : right;
                         const float2 sx = make_float2(__fadd_rn(xl, ctr.y), __fadd_rn(ctr.x, xr));
-                        const float2 ym = r > 0 ? A[lev - 1][r - 1][p] : up[p];
-                        const float2 yp = r < R - 1 ? A[lev - 1][r + 1][p] : dn[p];
-                        float2 v = upd3_sx2(c0v, c1v, ctr, sx, ym, yp, B[lev - 1][r][p], N[r][p]);
+                        const float2 ym = r > 0 ? Ap[lev - 1][r - 1][p] : up[p];
+                        const float2 yp = r < R - 1 ? Ap[lev - 1][r + 1][p] : dn[p];
+                        float2 v = upd3_sx2(c0v, c1v, ctr, sx, ym, yp, Bp[lev - 1][r][p], N[r][p]);
                         if (bpl != nullptr) v = add2(v, bv[p]);
                         if constexpr (!PER) {
                             const bool fr = zfix || ((fixy >> r) & 1u);
@@ -290,8 +290,8 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                 for (int r = 0; r < R; ++r)
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
-                        B[lev - 1][r][p] = A[lev - 1][r][p];
-                        A[lev - 1][r][p] = N[r][p];
+                        Bp[lev - 1][r][p] = Ap[lev - 1][r][p];
+                        Ap[lev - 1][r][p] = N[r][p];
                         N[r][p] = res[r][p];
                     }
             }
@@ -316,7 +316,9 @@ tb3d_bulk_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
                     }
                 }
             }
-        }
+            ++it;
+        };
+        for (int iz = z0 - K; iz < z1 + K; ++iz) step(iz, B, A);
     }
 
     // every plane this warp issued must land before the block exits (normally all were consumed)
