@@ -382,9 +382,10 @@ static cudaError_t march_k1_t(const Launch& L) {
     T* o = static_cast<T*>(L.out);
     const long long target = 8LL * sm_count();
     // defaults measured on a B200: in 3D the lean one-column-per-lane march (2.1-2.4x the
-    // vector march on unaligned grids); in 2D the raw-row march with 8 rows per step (16384^2:
-    // fp32 805 vs 674 GLUPS for the float-window march, bf16 1257 vs 547)
-    const int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : 3);
+    // vector march on unaligned grids); in 2D the raw-row march, 8 rows per step for fp32 and
+    // 6 for 16-bit storage (16384^2: fp32 805 vs 674 GLUPS for the float-window march, bf16
+    // 1289 vs 547)
+    const int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : (sizeof(T) == 4 ? 3 : 4));
     if (cfg == 0) {
         if (L.dims == 2) {
             constexpr int W = 4, RB = 4;
@@ -407,9 +408,9 @@ static cudaError_t march_k1_t(const Launch& L) {
         return cudaGetLastError();
     }
     if (L.dims == 2 && cfg >= 2 && vec_ok<T, PER, 16 / sizeof(T)>(L)) {
-        // raw-row march: 2 -> 4 rows per step, 3 -> 8 rows per step (4 warps per block)
+        // raw-row march: 2 -> 4 rows per step, 3 -> 8, 4 -> 6 (4 warps per block)
         constexpr int V = 16 / sizeof(T), W = 4;
-        const int rb = cfg == 2 ? 4 : 8;
+        const int rb = cfg == 2 ? 4 : (cfg == 4 ? 6 : 8);
         const int strips = cdiv(L.nx, 32 * V);
         // many short row chunks (about 64 rows at 16384^2, the measured best) keep more blocks
         // and loads in flight than one chunk per resident block
@@ -419,6 +420,9 @@ static cudaError_t march_k1_t(const Launch& L) {
         if (grd.y > 65535) return cudaErrorInvalidConfiguration;
         if (cfg == 2)
             march2d_raw_kernel<T, PER, W, 4><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.ny, L.nx,
+                                                                         L.c0, L.c1, ych);
+        else if (cfg == 4)
+            march2d_raw_kernel<T, PER, W, 6><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.ny, L.nx,
                                                                          L.c0, L.c1, ych);
         else
             march2d_raw_kernel<T, PER, W, 8><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.ny, L.nx,
@@ -517,13 +521,14 @@ cudaError_t launch_tb(const Launch& L) {
     return launch_tb_plain(L);
 }
 
-// 2D: 0 lean one-column-per-lane march, 1 float-window vector march, 2 / 3 raw-row vector march
-// with 4 / 8 rows per step (shapes without whole 16-byte rows fall back to 1). 3D: 0 lean, 1
+// 2D: 0 lean one-column-per-lane march, 1 float-window vector march, 2 / 3 / 4 raw-row vector
+// march with 4 / 8 / 6 rows per step (shapes without whole 16-byte rows fall back to 1). 3D: 0 lean, 1
 // vector march.
 int march_configs(int dims, const char** names, int max) {
-    static const char* k2[] = {"lane1_W4_RB4", "V16B_W4_RB4", "raw16B_W4_RB4", "raw16B_W4_RB8"};
+    static const char* k2[] = {"lane1_W4_RB4", "V16B_W4_RB4", "raw16B_W4_RB4", "raw16B_W4_RB8",
+                               "raw16B_W4_RB6"};
     static const char* k3[] = {"lane1_R4_W4", "V16B_R2_W8"};
-    const int n = dims == 2 ? 4 : 2;
+    const int n = dims == 2 ? 5 : 2;
     for (int i = 0; i < n && names != nullptr && i < max; ++i) names[i] = dims == 2 ? k2[i] : k3[i];
     return n;
 }
