@@ -46,6 +46,9 @@ struct ZmCfg {
     static constexpr int STAGE_BYTES = ((BODY_BYTES + 2 * SIDE_BYTES + 127) / 128) * 128;
     static constexpr int TX_BYTES = BODY_BYTES + 2 * SIDE_BYTES;  // bytes landed per plane
     static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 16;
+    // every box lands at a 128-byte aligned shared-memory address (the tensor-copy destination
+    // rule): rows are 512 bytes, and the second side box starts SIDE_BYTES after the first
+    static_assert(SIDE_BYTES % 128 == 0, "TY must be a multiple of 8");
     static constexpr int THREADS = 32 * (NWC + 1);
 };
 
