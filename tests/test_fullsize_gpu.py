@@ -58,7 +58,7 @@ def test_kernel_families_agree_at_1024_cubed(field, bc):
     ref = _run("b200/zmarch", field, st, 9)
     want = ref.get_tensor().clone()
     ref.close()
-    for key in ("b200/naive", "b200/tb4"):
+    for key in ("b200/naive", "b200/tb4", "b200/auto"):  # auto: tb4 from the table at 1024^3
         s = _run(key, field, st, 9)
         same = torch.equal(s.get_tensor(), want)
         s.close()

@@ -94,3 +94,11 @@ def test_report_lists_entries_and_choices():
     md = tune.report(t)
     assert "| `tb:3:float32:4:xlarge` | V4_R2_W16_S4 | 0 | 782.5 |" in md
     assert "| `3:float32:xlarge` (n=1024) | 717.4 | - | - | 782.5 | - | tb k=4 |" in md
+
+
+def test_committed_table_picks_tb4_for_1024_cubed_fp32():
+    """The committed table's b200/auto choice depends on the grid size (measured on a B200)."""
+    t = tune.Table.load(tune.DEFAULT_TABLE)
+    assert t.best_for(3, "float32", 1024 ** 3)["k"] == 4
+    assert t.best_for(3, "float32", 512 ** 3)["k"] == 1
+    assert t.best_for(2, "float32", 16384 ** 2)["k"] == 8
