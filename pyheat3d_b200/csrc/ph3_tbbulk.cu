@@ -395,6 +395,8 @@ struct TbEntry {
 const TbEntry kTbNames[] = {
     {2, "V4_R2_W16_S4"}, {2, "V4_R4_W8_S4"},  {3, "V4_R2_W16_S4"}, {3, "V4_R4_W8_S4"},
     {4, "V4_R2_W16_S4"}, {4, "V2_R2_W16_S6"}, {8, "V2_R2_W16_S6"}, {8, "V2_R4_W8_S6"},
+    // 64-row tiles of 8-byte lane vectors: less y overlap, more shuffles (fastest fp32 tb3)
+    {3, "V2_R4_W16_S4"}, {4, "V2_R4_W16_S4"},
 };
 
 template <typename T, bool PER>
@@ -404,8 +406,10 @@ cudaError_t tbbulk_dispatch(const Launch& L) {
         case 2:
             return cfg == 1 ? tbbulk_t<T, PER, 2, 4, 4, 8, 4>(L) : tbbulk_t<T, PER, 2, 4, 2, 16, 4>(L);
         case 3:
+            if (cfg == 2) return tbbulk_t<T, PER, 3, 2, 4, 16, 4>(L);
             return cfg == 1 ? tbbulk_t<T, PER, 3, 4, 4, 8, 4>(L) : tbbulk_t<T, PER, 3, 4, 2, 16, 4>(L);
         case 4:
+            if (cfg == 2) return tbbulk_t<T, PER, 4, 2, 4, 16, 4>(L);
             return cfg == 1 ? tbbulk_t<T, PER, 4, 2, 2, 16, 6>(L) : tbbulk_t<T, PER, 4, 4, 2, 16, 4>(L);
         case 8:
             return cfg == 1 ? tbbulk_t<T, PER, 8, 2, 4, 8, 6>(L) : tbbulk_t<T, PER, 8, 2, 2, 16, 6>(L);
