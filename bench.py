@@ -20,6 +20,9 @@ z-march kernel (``b200/zmarch``). One bench *step* is one solve of ``--time-step
   bounded sample of the same workload.
 - ``precision``, ``batching``, ``serving``: the defect-correction solve of the 256^3 Poisson
   problem, the 512-grid batch and the 2000 req/s request stream (``--no-…`` flags skip them).
+- ``zslab``: one (512 N) x 512 x 512 grid split in z over the N ranks (halo exchange + z-range
+  z-march per step); on one GPU by default (halos by local copies), across ranks with
+  ``--zslab on``.
 
 ``--impl reference`` times the reference's CPU path (the NumPy oracle, thread-chunked over
 z-slabs with every host core) on the same workload and prints the same line with
@@ -66,6 +69,9 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-batch", action="store_true", help="skip the batching measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--no-precision", action="store_true", help="skip the precision measurement")
+    ap.add_argument("--zslab", default="auto", choices=("auto", "on", "off"),
+                    help="z-slab split measurement: auto runs it on one GPU only (halos by "
+                         "local copies); on also runs it across ranks (NCCL halo exchange)")
     ap.add_argument("--serve-seconds", type=float, default=5.0,
                     help="length of the Poisson request stream (2000 req/s)")
     ap.add_argument("--variant", default="b200/zmarch",
@@ -410,6 +416,10 @@ def run_b200(a: argparse.Namespace) -> None:
                                "(pyheat3d numpy/slicing)"}
 
     extra = {}
+    if a.zslab == "on" or (a.zslab == "auto" and ws == 1):
+        # every rank takes part (collectives in the same order on all ranks), no try/except
+        extra["zslab"] = bench_zslab(torch, ws, rank, min(T, 200), value / ws)
+        torch.cuda.empty_cache()
     if ws == 1:
         for name, flag, fn in (("precision", a.no_precision, lambda: bench_precision(torch)),
                                ("batching", a.no_batch, lambda: bench_batching(torch)),
@@ -456,6 +466,41 @@ def run_b200(a: argparse.Namespace) -> None:
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------
+# z-slab split of one grid over the ranks
+# ---------------------------------------------------------------------------------------------
+def bench_zslab(torch, ws: int, rank: int, tsteps: int, per_rank_glups: float) -> dict:
+    """One (512 N) x 512 x 512 fp32 periodic grid split in z over the N ranks (512 planes each):
+    per step a halo exchange and the z-range z-march; device time of `tsteps` steps, max over
+    ranks. With one rank the periodic halos are local plane copies."""
+    from pyheat3d_b200 import heat_stencil
+    from pyheat3d_b200.slab import SlabSplit, SlabStepper
+
+    split = SlabSplit(N3 * ws, ws, True)
+    slab = np.zeros((N3 + 2, N3, N3), dtype=np.float32)
+    slab[1:-1] = field(N3, 3, seed=rank)  # halos arrive with the first exchange
+    st = SlabStepper(slab, heat_stencil(3, R3, "periodic"), split, rank)
+    del slab
+    st.step(20)
+    barrier(torch, ws)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    st.step(tsteps)
+    e.record()
+    e.synchronize()
+    secs = max_over_ranks(torch, ws, s.elapsed_time(e) * 1e-3)
+    barrier(torch, ws)
+    glups = split.nz * N3 * N3 * tsteps / secs / 1e9
+    finite = bool(torch.isfinite(st.owned()).all().item())
+    del st
+    return {"grid": [split.nz, N3, N3], "ranks": ws, "bc": "periodic", "storage": "float32",
+            "time_steps": tsteps, "glups": round(glups, 2),
+            "ms_per_update": round(secs / tsteps * 1e3, 4),
+            "exchange": "local plane copies" if ws == 1 else "NCCL send/recv of halo planes",
+            "vs_whole_grid_per_rank": round(glups / ws / per_rank_glups, 4),
+            "finite": finite}
 
 
 # ---------------------------------------------------------------------------------------------

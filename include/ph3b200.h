@@ -91,6 +91,19 @@ int ph3_zmarch3d(const void* u, void* out, const float* src, int nz, int ny, int
                  float c1, int storage, int bc, int chunk, void* stream);
 
 /*
+ * One update of the planes z0 .. z1-1 only (1 <= z0 <= z1 <= nz-1), reading planes z0-1 .. z1:
+ * the z-march of ph3_zmarch3d restricted to a range of planes, with no wrap in z; `bc` applies
+ * to x and y (Dirichlet also leaves the outer rows and columns of every plane unwritten). This
+ * is the kernel of a z-slab split of one grid over several GPUs: a rank's array holds its slab
+ * between two halo planes that the caller refreshes before each step (with periodic x / y for a
+ * periodic grid). Planes outside the range are not written. No counterpart in the reference,
+ * which runs one grid on one GPU (cupy_backend.py:188-194).
+ */
+int ph3_zmarch3d_planes(const void* u, void* out, const float* src, int nz, int ny, int nx,
+                        int z0, int z1, float c0, float c1, int storage, int bc, int chunk,
+                        void* stream);
+
+/*
  * One update by the 2D y-march. Replaces stencil.cu:289-385 tb2d with K = 1 ("ymarch",
  * cupy_backend.py:63-70). `chunk` = rows per block (<= 0: default).
  */

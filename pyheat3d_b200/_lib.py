@@ -26,6 +26,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "ph3_naive2d": (_i, [_p, _p, _p, _i, _i, _f, _f, _i, _i, _p]),
     "ph3_naive3d": (_i, [_p, _p, _p, _i, _i, _i, _f, _f, _i, _i, _p]),
     "ph3_zmarch3d": (_i, [_p, _p, _p, _i, _i, _i, _f, _f, _i, _i, _i, _p]),
+    "ph3_zmarch3d_planes": (_i, [_p, _p, _p, _i, _i, _i, _i, _i, _f, _f, _i, _i, _i, _p]),
     "ph3_ymarch2d": (_i, [_p, _p, _p, _i, _i, _f, _f, _i, _i, _i, _p]),
     "ph3_tb3d": (_i, [_p, _p, _p, _i, _i, _i, _i, _f, _f, _i, _i, _i, _p]),
     "ph3_tb2d": (_i, [_p, _p, _p, _i, _i, _i, _f, _f, _i, _i, _i, _p]),

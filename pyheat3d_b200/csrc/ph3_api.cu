@@ -113,6 +113,7 @@ Launch make(int dims, int nz, int ny, int nx, int storage, int bc, float c0, flo
     L.dims = dims; L.nz = dims == 2 ? 1 : nz; L.ny = ny; L.nx = nx;
     L.periodic = bc == PH3_PERIODIC; L.storage = storage;
     L.c0 = c0; L.c1 = c1; L.k = k; L.chunk = chunk; L.cfg = -1;
+    L.zb = 0; L.ze = 0;
     L.stream = static_cast<cudaStream_t>(stream);
     L.err = status_ptr();
     return L;
@@ -233,6 +234,22 @@ int ph3_zmarch3d(const void* u, void* out, const float* src, int nz, int ny, int
                                      stream),
                                 PH3_VARIANT_MARCH),
                   "zmarch3d launch");
+}
+
+int ph3_zmarch3d_planes(const void* u, void* out, const float* src, int nz, int ny, int nx,
+                        int z0, int z1, float c0, float c1, int storage, int bc, int chunk,
+                        void* stream) {
+    int rc = check_grid(3, nz, ny, nx, storage, bc);
+    if (rc == PH3_OK) rc = check_ptrs(u, out, src);
+    if (rc != PH3_OK) return rc;
+    if (z0 < 1 || z1 > nz - 1 || z0 > z1)
+        return fail(PH3_EINVAL, "planes [%d, %d) must satisfy 1 <= z0 <= z1 <= nz-1 = %d", z0, z1,
+                    nz - 1);
+    if (z0 == z1) return finish(cudaSuccess, "");
+    Launch L = make(3, nz, ny, nx, storage, bc, c0, c1, u, out, src, 1, chunk, stream);
+    L.zb = z0;
+    L.ze = z1;
+    return finish(launch_single(L, PH3_VARIANT_MARCH), "zmarch3d_planes launch");
 }
 
 int ph3_ymarch2d(const void* u, void* out, const float* src, int ny, int nx, float c0, float c1,

@@ -23,6 +23,8 @@ struct Launch {
     int k;              // fused time steps (1 for single-step kernels)
     int chunk;          // march chunk length (planes in 3D, rows in 2D); <= 0 picks a default
     int cfg;            // compiled tile configuration of the family; < 0 picks the default
+    int zb, ze;         // 3D single step: update only planes zb .. ze-1, no wrap in z (ze > 0;
+                        // 1 <= zb <= ze <= nz-1); ze == 0: every plane the boundary allows
     cudaStream_t stream;
     int* err;           // device status word for bounded waits (may be null)
 };

@@ -320,11 +320,11 @@ tb2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict_
 template <typename T, bool PER, int R, int W>
 __global__ void __launch_bounds__(32 * W)
 lite3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
-              int ny, int nx, float c0, float c1, int zch) {
+              int ny, int nx, float c0, float c1, int zch, int zb, int ze) {
     const int w = threadIdx.x >> 5;
-    const int z0 = blockIdx.z * zch;
+    const int z0 = zb + blockIdx.z * zch;
     lite3d_item<T, PER, R, false>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x,
-                                  (blockIdx.y * W + w) * R, z0, min(z0 + zch, nz));
+                                  (blockIdx.y * W + w) * R, z0, min(z0 + zch, ze));
 }
 
 template <typename T, bool PER, int RB, int W>
@@ -385,7 +385,8 @@ static cudaError_t march_k1_t(const Launch& L) {
     // vector march on unaligned grids); in 2D the raw-row march, 8 rows per step for fp32 and
     // 6 for 16-bit storage (16384^2: fp32 805 vs 674 GLUPS for the float-window march, bf16
     // 1289 vs 547)
-    const int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : (sizeof(T) == 4 ? 3 : 4));
+    int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : (sizeof(T) == 4 ? 3 : 4));
+    if (L.ze > 0) cfg = 0;  // z ranges: the lean march only
     if (cfg == 0) {
         if (L.dims == 2) {
             constexpr int W = 4, RB = 4;
@@ -398,12 +399,14 @@ static cudaError_t march_k1_t(const Launch& L) {
                                                                       L.c0, L.c1, ych);
         } else {
             constexpr int R = 4, W = 4;
+            // planes zb .. ze-1 (a z range never wraps: its neighbour planes are in the array)
+            const int zb = L.ze > 0 ? L.zb : 0, ze = L.ze > 0 ? L.ze : L.nz;
             const long long tiles = 1LL * cdiv(L.nx, 32) * cdiv(L.ny, W * R);
-            const int zch = L.chunk > 0 ? L.chunk : default_chunk(L.nz, tiles, 16, 2 * target);
-            dim3 grd(cdiv(L.nx, 32), cdiv(L.ny, W * R), cdiv(L.nz, zch));
+            const int zch = L.chunk > 0 ? L.chunk : default_chunk(ze - zb, tiles, 16, 2 * target);
+            dim3 grd(cdiv(L.nx, 32), cdiv(L.ny, W * R), cdiv(ze - zb, zch));
             if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
-            lite3d_kernel<T, PER, R, W><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.nz, L.ny,
-                                                                     L.nx, L.c0, L.c1, zch);
+            lite3d_kernel<T, PER, R, W><<<grd, 32 * W, 0, L.stream>>>(
+                u, o, L.src, L.nz, L.ny, L.nx, L.c0, L.c1, zch, zb, ze);
         }
         return cudaGetLastError();
     }

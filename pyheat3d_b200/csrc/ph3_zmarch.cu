@@ -617,6 +617,10 @@ cudaError_t zmarch_t(const Launch& L) {
     g.nty = (L.ny + TY - 1) / TY;
     g.zbase = L.periodic ? 0 : 1;
     g.nzi = L.periodic ? L.nz : L.nz - 2;
+    if (L.ze > 0) {  // a z range: planes zb-1 .. ze are inside the array, nothing wraps in z
+        g.zbase = L.zb;
+        g.nzi = L.ze - L.zb;
+    }
     if (g.nzi <= 0) return cudaSuccess;
     const long long tiles = 1LL * g.ntx * g.nty;
     const long long resident = 1LL * sm_count() * blocks_per_sm[dev];
