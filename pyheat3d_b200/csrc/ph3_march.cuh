@@ -518,6 +518,168 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// 3D single step for any row alignment with four columns per lane. A lane owns the columns
+// gx .. gx+3 (gx = x0 + 4 lane), a warp R rows of a 128-column strip. Every row access moves
+// the lane's four elements with the widest accesses the row's alignment allows: the element
+// index of gx from the array base modulo 4 is the same for every lane of a row, so one warp-
+// uniform branch picks one 4-element vector (residue 0), two pairs (2) or four scalars (odd).
+// Requires array bases aligned to 4 elements (16 bytes fp32, 8 bytes 16-bit). The last strip
+// of a row, when partial, reads per-element columns wrapped (periodic) or clamped (Dirichlet),
+// so lanes past the row end hold the neighbours the shuffles need; only in-row columns are
+// written. Planes rotate through three register sets by name, one plane in flight.
+// ------------------------------------------------------------------------------------------
+template <typename T, bool CG>
+__device__ __forceinline__ void ld4a(const T* __restrict__ p, int a, float (&v)[4]) {
+    if (a == 0) {
+        ld_vec<T, 4, CG>(p, v);
+    } else if (a == 2) {
+        float t[2], w[2];
+        ld_vec<T, 2, CG>(p, t);
+        ld_vec<T, 2, CG>(p + 2, w);
+        v[0] = t[0]; v[1] = t[1]; v[2] = w[0]; v[3] = w[1];
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = ldx1<CG>(p + j);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void st4a(T* __restrict__ p, int a, const float (&v)[4]) {
+    if (a == 0) {
+        st_vec<T, 4>(p, v);
+    } else if (a == 2) {
+        const float t[2] = {v[0], v[1]}, w[2] = {v[2], v[3]};
+        st_vec<T, 2>(p, t);
+        st_vec<T, 2>(p + 2, w);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) p[j] = from_f<T>(v[j]);
+    }
+}
+
+template <typename T, bool PER, int R, bool CG>
+__device__ __forceinline__ void avec3d_item(const T* __restrict__ u, T* __restrict__ o,
+                                            const float* __restrict__ b, int nz, int ny, int nx,
+                                            float c0, float c1, int strip, int row0, int zlo,
+                                            int zhi) {
+    constexpr int V = 4, EX = 32 * V;
+    const int lane = threadIdx.x & 31;
+    const int x0 = strip * EX, gx = x0 + lane * V;
+    if (x0 >= nx || row0 >= ny) return;  // warp-uniform
+    if constexpr (!PER) { zlo = max(zlo, 1); zhi = min(zhi, nz - 1); }
+    if (zlo >= zhi) return;
+    const int64_t P = int64_t(nx) * ny;
+    const bool full = x0 + EX <= nx;  // warp-uniform: all 128 columns inside the row
+    int cx[V];                        // per-element columns of a partial strip
+#pragma unroll
+    for (int j = 0; j < V; ++j) cx[j] = fix_idx<PER>(gx + j, nx);
+    const int hcol = lane == 0 ? fix_idx<PER>(x0 - 1, nx) : fix_idx<PER>(x0 + EX, nx);
+    const bool hl = lane == 0 || lane == 31;
+    int roff[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) roff[r] = fix_idx<PER>(row0 + r, ny) * nx;
+    const int uoff = fix_idx<PER>(row0 - 1, ny) * nx, doff = fix_idx<PER>(row0 + R, ny) * nx;
+    uint32_t skipx = 0, yskip = 0;  // columns / rows this lane must not write
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+        if (gx + j >= nx || (!PER && (gx + j == 0 || gx + j == nx - 1))) skipx |= 1u << j;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (row0 + r >= ny || (!PER && (row0 + r == 0 || row0 + r == ny - 1))) yskip |= 1u << r;
+    // residue modulo 4 of an element index (the array bases are 4-element aligned)
+    const int P4 = int(P & 3), x4 = x0 & 3;
+    auto res = [&](int z, int off) { return (z * P4 + off + x4) & 3; };
+    auto row4 = [&](const T* rp, int a, float (&v)[V]) {
+        if (full) {
+            ld4a<T, CG>(rp + gx, a, v);
+        } else {
+#pragma unroll
+            for (int j = 0; j < V; ++j) v[j] = ldx1<CG>(rp + cx[j]);
+        }
+    };
+
+    struct Plane {
+        float v[R][V], h[R];  // own rows; halo column (lanes 0 / 31)
+        float up[V], dn[V];   // rows above / below the warp's rows
+    };
+    auto load = [&](int z, Plane& p) {
+        const int zz = fix_near<PER>(z, nz);
+        const T* pl = u + int64_t(zz) * P;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            row4(pl + roff[r], res(zz, roff[r]), p.v[r]);
+            p.h[r] = hl ? ldx1<CG>(pl + roff[r] + hcol) : 0.f;
+        }
+        row4(pl + uoff, res(zz, uoff), p.up);
+        row4(pl + doff, res(zz, doff), p.dn);
+    };
+    float bel[R][V];
+    {
+        const int zz = fix_near<PER>(zlo - 1, nz);
+        const T* pl = u + int64_t(zz) * P;
+#pragma unroll
+        for (int r = 0; r < R; ++r) row4(pl + roff[r], res(zz, roff[r]), bel[r]);
+    }
+    Plane A, B, C;
+    load(zlo, A);
+    load(zlo + 1, B);
+    auto step = [&](int z, const Plane& ctr, const Plane& abv, Plane& pre) -> bool {
+        const bool more = z + 1 < zhi;
+        if (more) load(z + 2, pre);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float left = __shfl_up_sync(kFull, ctr.v[r][V - 1], 1);
+            const float right = __shfl_down_sync(kFull, ctr.v[r][0], 1);
+            const int gy = row0 + r;
+            // residue of this row's elements (roff[r] == gy * nx for every written row; the
+            // source is read at the same, possibly wrapped, row)
+            const int a = res(z, roff[r]);
+            float bv[V];
+            if (b != nullptr) {
+                const float* bp = b + int64_t(z) * P + int64_t(roff[r]);
+                if (full) {
+                    ld4a<float, false>(bp + gx, a, bv);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < V; ++j) bv[j] = __ldg(bp + cx[j]);
+                }
+            }
+            float out[V];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                const float xm = j > 0 ? ctr.v[r][j - 1] : (lane == 0 ? ctr.h[r] : left);
+                const float xp = j < V - 1 ? ctr.v[r][j + 1] : (lane == 31 ? ctr.h[r] : right);
+                const float ym = r > 0 ? ctr.v[r - 1][j] : ctr.up[j];
+                const float yp = r < R - 1 ? ctr.v[r + 1][j] : ctr.dn[j];
+                float v = upd3(c0, c1, ctr.v[r][j], xm, xp, ym, yp, bel[r][j], abv.v[r][j]);
+                if (b != nullptr) v = __fadd_rn(v, bv[j]);
+                out[j] = v;
+            }
+            if (!((yskip >> r) & 1u)) {
+                T* dst = o + int64_t(z) * P + int64_t(gy) * nx + gx;
+                if (skipx == 0) {
+                    st4a<T>(dst, a, out);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < V; ++j)
+                        if (!((skipx >> j) & 1u)) dst[j] = from_f<T>(out[j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int j = 0; j < V; ++j) bel[r][j] = ctr.v[r][j];
+        return more;
+    };
+    for (int z = zlo;;) {
+        if (!step(z++, A, B, C)) break;
+        if (!step(z++, B, C, A)) break;
+        if (!step(z++, C, A, B)) break;
+    }
+}
+
 template <typename T, bool PER, int RB, bool CG>
 __device__ __forceinline__ void lite2d_item(const T* __restrict__ u, T* __restrict__ o,
                                             const float* __restrict__ b, int ny, int nx,

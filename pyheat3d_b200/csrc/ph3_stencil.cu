@@ -327,6 +327,16 @@ lite3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restric
                                   (blockIdx.y * W + w) * R, z0, min(z0 + zch, ze));
 }
 
+template <typename T, bool PER, int R, int W>
+__global__ void __launch_bounds__(32 * W)
+avec3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
+              int ny, int nx, float c0, float c1, int zch, int zb, int ze) {
+    const int w = threadIdx.x >> 5;
+    const int z0 = zb + blockIdx.z * zch;
+    avec3d_item<T, PER, R, false>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x,
+                                  (blockIdx.y * W + w) * R, z0, min(z0 + zch, ze));
+}
+
 template <typename T, bool PER, int RB, int W>
 __global__ void __launch_bounds__(32 * W)
 lite2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int ny,
@@ -386,7 +396,28 @@ static cudaError_t march_k1_t(const Launch& L) {
     // 6 for 16-bit storage (16384^2: fp32 805 vs 674 GLUPS for the float-window march, bf16
     // 1289 vs 547)
     int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : (sizeof(T) == 4 ? 3 : 4));
-    if (L.ze > 0) cfg = 0;  // z ranges: the lean march only
+    if (L.dims == 3 && (cfg == 2 || cfg == 3)) {
+        // any-alignment lane vectors: 4 columns per lane; array bases aligned to 4 elements
+        if (aligned_to(L.u, 4 * sizeof(T)) && aligned_to(L.out, 4 * sizeof(T)) &&
+            aligned_to(L.src, 16)) {
+            constexpr int W = 4;
+            const int R = cfg == 2 ? 4 : 2;
+            const int zb = L.ze > 0 ? L.zb : 0, ze = L.ze > 0 ? L.ze : L.nz;
+            const long long tiles = 1LL * cdiv(L.nx, 128) * cdiv(L.ny, W * R);
+            const int zch = L.chunk > 0 ? L.chunk : default_chunk(ze - zb, tiles, 16, 2 * target);
+            dim3 grd(cdiv(L.nx, 128), cdiv(L.ny, W * R), cdiv(ze - zb, zch));
+            if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
+            if (cfg == 2)
+                avec3d_kernel<T, PER, 4, W><<<grd, 32 * W, 0, L.stream>>>(
+                    u, o, L.src, L.nz, L.ny, L.nx, L.c0, L.c1, zch, zb, ze);
+            else
+                avec3d_kernel<T, PER, 2, W><<<grd, 32 * W, 0, L.stream>>>(
+                    u, o, L.src, L.nz, L.ny, L.nx, L.c0, L.c1, zch, zb, ze);
+            return cudaGetLastError();
+        }
+        cfg = 0;
+    }
+    if (L.ze > 0) cfg = 0;  // z ranges: the lean march or the lane-vector march above
     if (cfg == 0) {
         if (L.dims == 2) {
             constexpr int W = 4, RB = 4;
@@ -525,13 +556,13 @@ cudaError_t launch_tb(const Launch& L) {
 }
 
 // 2D: 0 lean one-column-per-lane march, 1 float-window vector march, 2 / 3 / 4 raw-row vector
-// march with 4 / 8 / 6 rows per step (shapes without whole 16-byte rows fall back to 1). 3D: 0 lean, 1
-// vector march.
+// march with 4 / 8 / 6 rows per step (shapes without whole 16-byte rows fall back to 1). 3D: 0 lean,
+// 1 vector march, 2 / 3 any-alignment lane vectors with 4 / 2 rows per warp.
 int march_configs(int dims, const char** names, int max) {
     static const char* k2[] = {"lane1_W4_RB4", "V16B_W4_RB4", "raw16B_W4_RB4", "raw16B_W4_RB8",
                                "raw16B_W4_RB6"};
-    static const char* k3[] = {"lane1_R4_W4", "V16B_R2_W8"};
-    const int n = dims == 2 ? 5 : 2;
+    static const char* k3[] = {"lane1_R4_W4", "V16B_R2_W8", "V4any_R4_W4", "V4any_R2_W4"};
+    const int n = dims == 2 ? 5 : 4;
     for (int i = 0; i < n && names != nullptr && i < max; ++i) names[i] = dims == 2 ? k2[i] : k3[i];
     return n;
 }

@@ -269,7 +269,12 @@ def test_every_compiled_config(storage, bc):
     u2 = rng.random((41, 1160), dtype=np.float32)
     st2 = heat_stencil(2, 0.95 / 4, bc)
     u3 = rng.random((13, 21, 97), dtype=np.float32)
-    marches = [(2, u2, st2, "b200/ymarch" + suf), (3, u3, st, "b200/zmarch" + suf)]
+    # rows longer than one 128-column strip whose element residues modulo 4 cycle through
+    # 0..3 (nx = 261) or 0 / 2 (nx = 258): every access width of the lane-vector march
+    u3b = rng.random((7, 10, 261), dtype=np.float32)
+    u3c = rng.random((6, 9, 258), dtype=np.float32)
+    marches = [(2, u2, st2, "b200/ymarch" + suf), (3, u3, st, "b200/zmarch" + suf),
+               (3, u3b, st, "b200/zmarch" + suf), (3, u3c, st, "b200/zmarch" + suf)]
     try:
         for fam, k, key in cases:
             for cfg in range(L.ph3_tune_count(K[fam], 3, k)):
@@ -279,10 +284,14 @@ def test_every_compiled_config(storage, bc):
                     _assert_same(_run(key, u0, st, steps), _ref(key, u0, st, steps),
                                  (key, cfg, chunk))
         for dims, u, stc, key in marches:
+            bsrc = rng.random(u.shape, dtype=np.float32) if dims == 3 else None
             for cfg in range(L.ph3_tune_count(K["march"], dims, 1)):
                 for chunk in (0, 7):
                     _lib.check(L.ph3_tune_set(K["march"], dims, S, 1, cfg, chunk))
                     _assert_same(_run(key, u, stc, 5), _ref(key, u, stc, 5), (key, cfg, chunk))
+                if bsrc is not None:  # the Jacobi source through every 3D configuration
+                    _assert_same(_run(key, u, stc, 3, bsrc), _ref(key, u, stc, 3, bsrc),
+                                 (key, cfg, "source"))
     finally:
         for fam, k, _ in cases:
             L.ph3_tune_set(K[fam], 3, S, k, -1, 0)
