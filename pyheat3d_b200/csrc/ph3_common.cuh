@@ -335,6 +335,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, 
         : "memory");
 }
 
+// 1D tiled tensor load (x must be a multiple of 16 bytes' worth of elements; out-of-range parts
+// of the box, including negative coordinates, arrive as zeros).
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* tmap, int x, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.1d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2}], [%3];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(smem_u32(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y,
                                             uint64_t* bar) {
     asm volatile(

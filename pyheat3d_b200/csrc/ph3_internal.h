@@ -35,6 +35,9 @@ cudaError_t launch_march_k1(const Launch& L);   // register march, k = 1, any sh
 cudaError_t launch_tb(const Launch& L);         // temporal blocking, k in {2,3,4,8}
 cudaError_t launch_zmarch_tma(const Launch& L); // 3D TMA z-march, k = 1, aligned shapes
 bool zmarch_tma_supported(const Launch& L);
+// 3D single step for any nx from 1D tensor copies of row boxes (ph3_zmarch.cu); variant 0..2
+cudaError_t launch_ring3d(const Launch& L, int variant);
+bool ring3d_supported(const Launch& L);
 cudaError_t launch_tbbulk(const Launch& L);     // 3D tb with a bulk-copy ring, aligned shapes
 bool tbbulk_supported(const Launch& L);
 int tbbulk_configs(int k, const char** names, int max);

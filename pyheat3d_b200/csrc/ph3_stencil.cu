@@ -396,6 +396,11 @@ static cudaError_t march_k1_t(const Launch& L) {
     // 6 for 16-bit storage (16384^2: fp32 805 vs 674 GLUPS for the float-window march, bf16
     // 1289 vs 547)
     int cfg = L.cfg >= 0 ? L.cfg : (L.dims == 3 ? 0 : (sizeof(T) == 4 ? 3 : 4));
+    if (L.dims == 3 && cfg >= 4 && cfg <= 6) {
+        // row boxes by 1D tensor copies into per-warp shared-memory rings
+        if (ring3d_supported(L)) return launch_ring3d(L, cfg - 4);
+        cfg = 0;
+    }
     if (L.dims == 3 && (cfg == 2 || cfg == 3)) {
         // any-alignment lane vectors: 4 columns per lane; array bases aligned to 4 elements
         if (aligned_to(L.u, 4 * sizeof(T)) && aligned_to(L.out, 4 * sizeof(T)) &&
@@ -557,12 +562,14 @@ cudaError_t launch_tb(const Launch& L) {
 
 // 2D: 0 lean one-column-per-lane march, 1 float-window vector march, 2 / 3 / 4 raw-row vector
 // march with 4 / 8 / 6 rows per step (shapes without whole 16-byte rows fall back to 1). 3D: 0 lean,
-// 1 vector march, 2 / 3 any-alignment lane vectors with 4 / 2 rows per warp.
+// 1 vector march, 2 / 3 any-alignment lane vectors with 4 / 2 rows per warp, 4 / 5 / 6 row boxes
+// by 1D tensor copies into per-warp rings (rows per warp, ring stages: 2/3, 2/4, 4/3).
 int march_configs(int dims, const char** names, int max) {
     static const char* k2[] = {"lane1_W4_RB4", "V16B_W4_RB4", "raw16B_W4_RB4", "raw16B_W4_RB8",
                                "raw16B_W4_RB6"};
-    static const char* k3[] = {"lane1_R4_W4", "V16B_R2_W8", "V4any_R4_W4", "V4any_R2_W4"};
-    const int n = dims == 2 ? 5 : 4;
+    static const char* k3[] = {"lane1_R4_W4", "V16B_R2_W8", "V4any_R4_W4", "V4any_R2_W4",
+                               "ring1d_R2_W4_S3", "ring1d_R2_W4_S4", "ring1d_R4_W4_S3"};
+    const int n = dims == 2 ? 5 : 7;
     for (int i = 0; i < n && names != nullptr && i < max; ++i) names[i] = dims == 2 ? k2[i] : k3[i];
     return n;
 }

@@ -27,6 +27,7 @@
 
 #include "ph3_common.cuh"
 #include "ph3_internal.h"
+#include "ph3_march.cuh"
 
 namespace ph3 {
 
@@ -547,6 +548,265 @@ zmarch_v1_kernel(const __grid_constant__ CUtensorMap tm_body,
 }
 
 // ---------------------------------------------------------------------------------------------
+// 3D single step for rows without 16-byte vectors (any nx), fed by 1D tensor copies.
+//
+// The field is addressed as one flat array. A warp owns R rows of a 128-column strip (lane l:
+// columns x0 + 4l .. +3) and a z-chunk, with its own STAGES-deep shared-memory ring: per plane
+// one lane copies R + 2 rows (the warp's rows and the rows above and below) as 1D boxes of SPAN
+// elements that start at the 16-byte boundary at or before column x0 - 1, so every box starts
+// aligned whatever nx is; out-of-range parts of a box (before the first or after the last
+// element of the array) arrive as zeros. Lanes read their four columns at the row's offset in
+// the box with the widest shared-memory access the offset allows. Periodic strips at a row end
+// take the wrapped neighbour column from a 16-byte box around it. The own rows of planes z-1,
+// z, z+1 stay in registers; the ring keeps STAGES - 2 planes in flight. Every warp runs its own
+// pipeline (no block barrier) and every wait is bounded.
+// ---------------------------------------------------------------------------------------------
+template <typename T, bool PER, int R, int STAGES>
+struct RgCfg {
+    static constexpr int E = 16 / int(sizeof(T));          // elements per 16 bytes
+    static constexpr int NCH = (130 + 2 * (E - 1)) / E;     // 16-byte chunks per row box
+    static constexpr int SPAN = NCH * E;                    // elements per row box
+    static_assert(SPAN >= 130 + E - 1, "a row box covers x0-1 .. x0+128 at any offset");
+    static constexpr int ROWB = (SPAN * int(sizeof(T)) + 127) / 128 * 128;  // 128-byte slots
+    static constexpr int HALB = 128;                        // slot of one 16-byte halo box
+    static constexpr int NHAL = PER ? 2 * R : 0;            // left / right halo of each own row
+    static constexpr int STAGEB = (R + 2) * ROWB + NHAL * HALB;
+    static constexpr int WARPB = STAGES * STAGEB + 128;     // + the warp's mbarriers
+};
+
+template <typename T>
+__device__ __forceinline__ void lds4a(const T* p, int a, float (&v)[4]) {
+    if (a == 0) {
+        ld_vec_shared<T, 4>(p, v);
+    } else if (a == 2) {
+        float t[2], w[2];
+        ld_vec_shared<T, 2>(p, t);
+        ld_vec_shared<T, 2>(p + 2, w);
+        v[0] = t[0]; v[1] = t[1]; v[2] = w[0]; v[3] = w[1];
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = to_f(p[j]);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void ldg4a(const T* p, int a, float (&v)[4]) {
+    if (a == 0) {
+        ld_vec<T, 4>(p, v);
+    } else if (a == 2) {
+        float t[2], w[2];
+        ld_vec<T, 2>(p, t);
+        ld_vec<T, 2>(p + 2, w);
+        v[0] = t[0]; v[1] = t[1]; v[2] = w[0]; v[3] = w[1];
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = to_f(__ldg(p + j));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void stg4a(T* p, int a, const float (&v)[4]) {
+    if (a == 0) {
+        st_vec<T, 4>(p, v);
+    } else if (a == 2) {
+        const float t[2] = {v[0], v[1]}, w[2] = {v[2], v[3]};
+        st_vec<T, 2>(p, t);
+        st_vec<T, 2>(p + 2, w);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) p[j] = from_f<T>(v[j]);
+    }
+}
+
+template <typename T, bool PER, int R, int W, int STAGES>
+__global__ void __launch_bounds__(32 * W)
+ring3d_kernel(const __grid_constant__ CUtensorMap tm_row, const __grid_constant__ CUtensorMap tm_hal,
+              T* __restrict__ o, const float* __restrict__ b, int nz, int ny, int nx, float c0,
+              float c1, int zch, int zb, int ze, int* err) {
+    using C = RgCfg<T, PER, R, STAGES>;
+    constexpr int E = C::E, V = 4;
+    static_assert(STAGES >= 3, "planes z and z+1 are held while z+2 is copied");
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* wbase = smem + warp * C::WARPB;
+    uint64_t* full = reinterpret_cast<uint64_t*>(wbase + STAGES * C::STAGEB);
+    const int x0 = blockIdx.x * 128, gx = x0 + lane * V;
+    const int row0 = (blockIdx.y * W + warp) * R;
+    int zlo = zb + blockIdx.z * zch, zhi = min(zlo + zch, ze);
+    if constexpr (!PER) { zlo = max(zlo, 1); zhi = min(zhi, nz - 1); }
+    if (x0 >= nx || row0 >= ny || zlo >= zhi) return;  // warp-uniform; no block barrier below
+    if (lane == 0) {
+        for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+
+    const int64_t P = int64_t(nx) * ny;
+    const uint32_t P32 = uint32_t(P);  // low bits of plane offsets (element offsets modulo E)
+    int yoff[R + 2];                    // element offsets of rows row0-1 .. row0+R in a plane
+#pragma unroll
+    for (int rr = 0; rr < R + 2; ++rr) yoff[rr] = fix_idx<PER>(row0 - 1 + rr, ny) * nx;
+    const bool hleft = PER && x0 == 0, hright = PER && x0 + 128 >= nx;
+    const int nhal = (hleft ? R : 0) + (hright ? R : 0);
+    const uint32_t tx_bytes = uint32_t((R + 2) * C::SPAN * int(sizeof(T)) + nhal * 16);
+    uint32_t skipx = 0, yskip = 0;  // columns / rows this lane must not write
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+        if (gx + j >= nx || (!PER && (gx + j == 0 || gx + j == nx - 1))) skipx |= 1u << j;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (row0 + r >= ny || (!PER && (row0 + r == 0 || row0 + r == ny - 1))) yskip |= 1u << r;
+    // the column nx-1 in the last strip of a periodic row: its right neighbour is column 0
+    const int cl = nx - 1 - x0;  // its position in the strip (valid when hright)
+
+    const int npl = zhi - zlo + 2;  // planes zlo-1 .. zhi, numbered 0 .. npl-1
+    int issued = 0;                  // planes whose copies were started (lane 0)
+    auto stage = [&](int i) { return wbase + (i % STAGES) * C::STAGEB; };
+    auto issue = [&](int i) {  // lane 0: plane number i into its stage
+        const int zz = fix_near<PER>(zlo - 1 + i, nz);
+        const int64_t zo = int64_t(zz) * P;
+        unsigned char* st = stage(i);
+        uint64_t* bar = &full[i % STAGES];
+        mbar_arrive_expect_tx(bar, tx_bytes);
+#pragma unroll
+        for (int rr = 0; rr < R + 2; ++rr) {
+            const int64_t e0 = zo + yoff[rr] + x0 - 1;
+            tma_load_1d(st + rr * C::ROWB, &tm_row, int(e0 & ~int64_t(E - 1)), bar);
+        }
+        if constexpr (PER) {
+            unsigned char* hs = st + (R + 2) * C::ROWB;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int64_t rs = zo + yoff[r + 1];
+                if (hleft)
+                    tma_load_1d(hs + (2 * r) * C::HALB, &tm_hal,
+                                int((rs + nx - 1) & ~int64_t(E - 1)), bar);
+                if (hright)
+                    tma_load_1d(hs + (2 * r + 1) * C::HALB, &tm_hal, int(rs & ~int64_t(E - 1)),
+                                bar);
+            }
+        }
+        issued = i + 1;
+    };
+    // offset of column x0 - 1 in the box of row rr of plane zz
+    auto off = [&](int zz, int rr) {
+        return int((uint32_t(zz) * P32 + uint32_t(yoff[rr] + x0 - 1)) & uint32_t(E - 1));
+    };
+    auto rowp = [&](const unsigned char* st, int rr) {
+        return reinterpret_cast<const T*>(st + rr * C::ROWB);
+    };
+    auto own_rows = [&](int i, float (&v)[R][V]) {  // the own rows' columns of plane number i
+        const int zz = fix_near<PER>(zlo - 1 + i, nz);
+        const unsigned char* st = stage(i);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int d = off(zz, r + 1);
+            lds4a<T>(rowp(st, r + 1) + d + 1 + 4 * lane, (d + 1) & 3, v[r]);
+        }
+    };
+    int waited = 0;  // planes seen to land by the whole warp
+    auto wait = [&](int i) {  // warp-uniform result, so the warp never splits at a shuffle
+        const bool r = mbar_wait(&full[i % STAGES], (uint32_t(i) / STAGES) & 1u, err);
+        const bool all = __all_sync(kFullMask, r);
+        if (all) waited = i + 1;
+        return all;
+    };
+
+    if (lane == 0)  // fill every stage; afterwards step z refills the stage of plane z-1
+        for (int i = 0; i < min(STAGES, npl); ++i) issue(i);
+    float bel[R][V], ctr[R][V], abv[R][V];
+    bool ok = wait(0);
+    if (ok) own_rows(0, bel);
+    ok = ok && wait(1);
+    if (ok) own_rows(1, ctr);
+    for (int z = zlo; ok && z < zhi; ++z) {
+        const int ic = z - zlo + 1;  // plane number of z
+        // refill the stage of plane z-1 (number ic-1), whose last reads were in the previous
+        // step, with plane number ic-1+STAGES
+        __syncwarp();
+        if (lane == 0 && ic - 1 + STAGES < npl) {
+            fence_proxy_async_smem();
+            issue(ic - 1 + STAGES);
+        }
+        if (!wait(ic + 1)) { ok = false; break; }
+        own_rows(ic + 1, abv);
+        const unsigned char* st = stage(ic);
+        float up[V], dn[V];
+        {
+            const int du = off(z, 0), dd = off(z, R + 1);
+            lds4a<T>(rowp(st, 0) + du + 1 + 4 * lane, (du + 1) & 3, up);
+            lds4a<T>(rowp(st, R + 1) + dd + 1 + 4 * lane, (dd + 1) & 3, dn);
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int d = off(z, r + 1);
+            const int a = (d + 1) & 3;  // residue of the row's columns (global and shared)
+            const T* rp = rowp(st, r + 1) + d;
+            const float left = __shfl_up_sync(kFullMask, ctr[r][V - 1], 1);
+            const float right = __shfl_down_sync(kFullMask, ctr[r][0], 1);
+            float xm[V], xp[V];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                xm[j] = j > 0 ? ctr[r][j - 1] : (lane == 0 ? to_f(rp[0]) : left);
+                xp[j] = j < V - 1 ? ctr[r][j + 1] : (lane == 31 ? to_f(rp[129]) : right);
+            }
+            if constexpr (PER) {
+                const T* hs = reinterpret_cast<const T*>(st + (R + 2) * C::ROWB +
+                                                         (2 * r) * C::HALB);
+                const uint32_t rs = uint32_t(z) * P32 + uint32_t(yoff[r + 1]);
+                if (hleft && lane == 0) xm[0] = to_f(hs[(rs + uint32_t(nx - 1)) & uint32_t(E - 1)]);
+                if (hright && lane == (cl >> 2)) {
+                    const float w = to_f(hs[C::HALB / int(sizeof(T)) + (rs & uint32_t(E - 1))]);
+#pragma unroll
+                    for (int j = 0; j < V; ++j)
+                        if (j == (cl & 3)) xp[j] = w;
+                }
+            }
+            float out[V];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                const float ym = r > 0 ? ctr[r - 1][j] : up[j];
+                const float yp = r < R - 1 ? ctr[r + 1][j] : dn[j];
+                out[j] = upd3(c0, c1, ctr[r][j], xm[j], xp[j], ym, yp, bel[r][j], abv[r][j]);
+            }
+            if (!((yskip >> r) & 1u)) {
+                const int64_t ro = int64_t(z) * P + int64_t(row0 + r) * nx + gx;
+                if (b != nullptr) {
+                    float bv[V];
+                    if (gx + V <= nx) {
+                        ldg4a<float>(b + ro, a, bv);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < V; ++j) bv[j] = gx + j < nx ? __ldg(b + ro + j) : 0.f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < V; ++j) out[j] = __fadd_rn(out[j], bv[j]);
+                }
+                if (skipx == 0) {
+                    stg4a<T>(o + ro, a, out);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < V; ++j)
+                        if (!((skipx >> j) & 1u)) o[ro + j] = from_f<T>(out[j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                bel[r][j] = ctr[r][j];
+                ctr[r][j] = abv[r][j];
+            }
+    }
+    if (!ok && lane == 0) {
+        // a wait expired: let the copies this warp started land before its shared memory goes
+        for (int i = waited; i < issued; ++i)
+            if (!mbar_wait(&full[i % STAGES], (uint32_t(i) / STAGES) & 1u, err)) break;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
@@ -582,6 +842,58 @@ bool make_map(CUtensorMap* m, const void* base, int nz, int ny, int nx, int bx, 
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T>
+bool make_map_1d(CUtensorMap* m, const void* base, uint64_t n, uint32_t box) {
+    auto enc = get_encode();
+    if (enc == nullptr) return false;
+    cuuint64_t dims[1] = {cuuint64_t(n)};
+    cuuint64_t strides[1] = {0};  // unused for rank 1
+    cuuint32_t bx[1] = {box};
+    cuuint32_t es[1] = {1};
+    return enc(m, tm_dtype<T>(), 1, const_cast<void*>(base), dims, strides, bx, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T, bool PER, int R, int W, int STAGES>
+cudaError_t ring3d_t(const Launch& L) {
+    using C = RgCfg<T, PER, R, STAGES>;
+    constexpr int SMEM = W * C::WARPB;
+    auto kern = ring3d_kernel<T, PER, R, W, STAGES>;
+    static bool attr_set[64] = {false};  // per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+        if (e != cudaSuccess) return e;
+        attr_set[dev] = true;
+    }
+    const uint64_t n = uint64_t(L.nz) * L.ny * L.nx;
+    CUtensorMap tr, th;
+    if (!make_map_1d<T>(&tr, L.u, n, C::SPAN) || !make_map_1d<T>(&th, L.u, n, C::E))
+        return cudaErrorInvalidValue;
+    const int zb = L.ze > 0 ? L.zb : 0, ze = L.ze > 0 ? L.ze : L.nz;
+    auto cd = [](long long a, long long b) { return int((a + b - 1) / b); };
+    const long long tiles = 1LL * cd(L.nx, 128) * cd(L.ny, W * R);
+    const int zch = L.chunk > 0 ? L.chunk : default_chunk(ze - zb, tiles, 16, 16LL * sm_count());
+    dim3 grd(cd(L.nx, 128), cd(L.ny, W * R), cd(ze - zb, zch));
+    if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
+    kern<<<grd, 32 * W, SMEM, L.stream>>>(tr, th, static_cast<T*>(L.out), L.src, L.nz, L.ny, L.nx,
+                                          L.c0, L.c1, zch, zb, ze, L.err);
+    return cudaGetLastError();
+}
+
+template <typename T, bool PER>
+cudaError_t ring3d_cfg(const Launch& L, int variant) {
+    switch (variant) {
+        case 0: return ring3d_t<T, PER, 2, 4, 3>(L);
+        case 1: return ring3d_t<T, PER, 2, 4, 4>(L);
+        default: return ring3d_t<T, PER, 4, 4, 3>(L);
+    }
 }
 
 // FORM: 0 the register-capped packed/scalar consumer, 1 the first scalar consumer.
@@ -684,6 +996,31 @@ static cudaError_t zmarch_cfg(const Launch& L) {
         case 6: return zmarch_t<T, PER, 16, 16, 6, false>(L);
         case 7: return zmarch_t<T, PER, 16, 8, 6, true, 1>(L);
         default: return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
+    }
+}
+
+bool ring3d_supported(const Launch& L) {
+    const size_t es = L.storage == kF32 ? 4 : 2;
+    auto al = [](const void* p, size_t a) {
+        return p == nullptr || reinterpret_cast<uintptr_t>(p) % a == 0;
+    };
+    const long long n = 1LL * L.nz * L.ny * L.nx;
+    return L.dims == 3 && n + 512 < (1LL << 31) && al(L.u, 16) && al(L.out, 4 * es) &&
+           al(L.src, 16) && get_encode() != nullptr;
+}
+
+cudaError_t launch_ring3d(const Launch& L, int variant) {
+    switch (L.storage) {
+        case kF32:
+            return L.periodic ? ring3d_cfg<float, true>(L, variant)
+                              : ring3d_cfg<float, false>(L, variant);
+        case kF16:
+            return L.periodic ? ring3d_cfg<__half, true>(L, variant)
+                              : ring3d_cfg<__half, false>(L, variant);
+        case kBF16:
+            return L.periodic ? ring3d_cfg<__nv_bfloat16, true>(L, variant)
+                              : ring3d_cfg<__nv_bfloat16, false>(L, variant);
+        default: return cudaErrorInvalidValue;
     }
 }
 
