@@ -467,7 +467,7 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
         float s[R];        // Jacobi source of the own rows (0 without a source)
     };
     auto load = [&](int z, Plane& p) {
-        const int64_t zo = int64_t(fix_idx<PER>(z, nz)) * P;
+        const int64_t zo = int64_t(fix_near<PER>(z, nz)) * P;
         const T* pl = u + zo;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -480,7 +480,7 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
     };
     float bel[R];
     {
-        const T* pl = u + int64_t(fix_idx<PER>(zlo - 1, nz)) * P;
+        const T* pl = u + int64_t(fix_near<PER>(zlo - 1, nz)) * P;
 #pragma unroll
         for (int r = 0; r < R; ++r) bel[r] = ldx1<CG>(pl + roff[r] + cx);
     }
@@ -697,7 +697,7 @@ __device__ __forceinline__ void lite2d_item(const T* __restrict__ u, T* __restri
     // two row windows used in turn (rows y-1 .. y+RB and their halo values): the next RB rows
     // load straight into the other window, so only the two overlap rows are ever copied
     float P[RB + 2], Ph[RB + 2], Q[RB + 2], Qh[RB + 2];
-    auto row = [&](int y) { return u + int64_t(fix_idx<PER>(y, ny)) * nx; };
+    auto row = [&](int y) { return u + int64_t(fix_near<PER>(y, ny)) * nx; };
 #pragma unroll
     for (int q = 0; q < RB + 2; ++q) {
         const T* rp = row(ylo - 1 + q);
