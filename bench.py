@@ -98,13 +98,14 @@ def peaks() -> tuple[float, str]:
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def workload_config(dims: int, n: int, storage: str, tsteps: int, ws: int) -> dict:
-    """The `config` object of both arms' JSON lines (the same workload; `time_steps_per_step`
-    is the part of a solve one bench step covers)."""
+def workload_config(dims: int, n: int, storage: str, ws: int) -> dict:
+    """The `config` object of both arms' JSON lines: the same workload on both. How many
+    updates one bench step covers is reported beside it (`time_steps_per_step`), since the CPU
+    arm times a bounded sample of the same solve."""
     return {"workload": f"{dims}D {n}^{dims} {storage} periodic heat, r=0.95/{2 * dims}, "
                         "uniform[0,1) fields, seed 0 (rank r: seed r)",
             "grid": [n] * dims, "bc": "periodic", "storage": storage,
-            "time_steps_per_step": tsteps, "units": "site updates (all cells)",
+            "units": "site updates (all cells)",
             "l2": f"inputs larger than L2 ({n ** dims * (4 if storage == 'float32' else 2) >> 20}"
                   " MiB field vs 126 MB L2)",
             "parallelism": f"replicas x{ws}"}
@@ -261,8 +262,28 @@ def time_solves(torch, st, nsolves: int, tsteps: int) -> float:
     return s.elapsed_time(e) * 1e-3
 
 
+def check_parity(st, u0: np.ndarray, stencil) -> dict:
+    """Run the stepper's kernel for max(2, k) updates of the bench field (one pass and a
+    remainder for tb<k>) and compare with the oracle (thread-chunked, bit-identical to
+    pyheat3d's reference_step / emulated_reference) bit for bit."""
+    from oracle import threaded_emulated
+
+    k = st.steps_per_pass
+    n = k + 1 if k > 1 else 2
+    st.step(n)
+    got = st.get()
+    want = threaded_emulated(u0, stencil.c0, stencil.c1, stencil.bc, n, st.storage,
+                             k if st.storage != "float32" else 1, threads=host_cores())
+    diff = int(np.count_nonzero(got != want))
+    err = float(np.abs(got.astype(np.float64) - want).max() / np.abs(want).max())
+    return {"steps": n, "oracle": "NumPy restatement of pyheat3d reference_step, all host "
+            "threads", "bitwise_equal": diff == 0, "mismatches": diff, "max_rel_err": err}
+
+
 def variant_row(torch, key: str, u0: np.ndarray, stencil, tsteps: int, copy_bw: float) -> dict:
     from pyheat3d_b200.registry import VARIANTS, make_stepper
+
+    from pyheat3d_b200.traffic import tb_model_bytes
 
     var = VARIANTS[key]
     st = make_stepper(key, u0, stencil)
@@ -270,13 +291,21 @@ def variant_row(torch, key: str, u0: np.ndarray, stencil, tsteps: int, copy_bw: 
     torch.cuda.synchronize()
     secs = time_solves(torch, st, 1, tsteps)
     ok = bool(np.isfinite(st.get_tensor().float().sum().item()))
+    tile = dict(st.tile)
     st.close()
     cells = u0.size
     glups = cells * tsteps / secs / 1e9
-    bpu = 2.0 * var.bytes_per_value / var.steps_per_pass
-    return {"glups": round(glups, 2), "bytes_per_update": bpu,
-            "effective_GBs": round(glups * bpu, 1), "frac_copy": round(glups * bpu / copy_bw, 4),
-            "k": var.steps_per_pass, "storage": var.storage, "finite": ok}
+    k = var.steps_per_pass
+    bpu = 2.0 * var.bytes_per_value / k
+    row = {"glups": round(glups, 2), "bytes_per_update": bpu,
+           "effective_GBs": round(glups * bpu, 1), "frac_copy": round(glups * bpu / copy_bw, 4),
+           "k": k, "storage": var.storage, "finite": ok}
+    if k > 1 and "tx" in tile:  # pyheat3d's halo-aware estimate (benchmark.py:219-230)
+        hb = tb_model_bytes(u0.ndim, k, var.bytes_per_value, tile["tx"], tile["ty"], tile["zch"])
+        row.update({"halo_model_bytes_per_unit": round(hb, 4),
+                    "halo_model_GBs": round(glups * hb, 1),
+                    "tile": [tile["tx"], tile["ty"], tile["zch"]]})
+    return row
 
 
 def cpu_sample(u0: np.ndarray, c0: float, c1: float, threads: int, sweeps: int) -> float:
@@ -324,8 +353,13 @@ def run_b200(a: argparse.Namespace) -> None:
     u0 = field(a.n, a.dims, seed=rank)
     cells = u0.size
 
-    # ---- value: K solves, field resident in HBM
+    # ---- parity first: the measured kernel on the measured field against the oracle
     st = make_stepper(a.variant, u0, stencil)
+    parity = check_parity(st, u0, stencil)
+    if not parity["bitwise_equal"]:
+        raise SystemExit(f"bench: {a.variant} differs from the oracle on the bench field: {parity}")
+
+    # ---- value: K solves, field resident in HBM
     for _ in range(W):
         st.step(T)
     barrier(torch, ws)
@@ -444,7 +478,8 @@ def run_b200(a: argparse.Namespace) -> None:
             "value": round(value, 2), "kernel": a.variant, "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": round(secs / K * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(a.dims, a.n, var.storage, T, ws),
+            "config": workload_config(a.dims, a.n, var.storage, ws),
+            "time_steps_per_step": T,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
                          "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                          "traffic": traffic, "peak_kind": peak_kind,
@@ -457,9 +492,10 @@ def run_b200(a: argparse.Namespace) -> None:
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
-            "variants": variants,
+            "parity": parity,
             **extra,
             "finite": final_ok,
+            "variants": variants,  # last: the longest part of the line
         }
         print(json.dumps(line))
     if ws > 1:
@@ -653,7 +689,8 @@ def run_reference(a: argparse.Namespace) -> None:
         "value": round(value, 4), "unit": "GLUPS", "n_gpus": ws, "steps": K, "warmup": W,
         "ms_per_step": round(secs / K * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(3, N3, "float32", sweeps, ws),
+        "config": workload_config(3, N3, "float32", ws),
+        "time_steps_per_step": sweeps,
         "cpu_baseline": {"value": round(value, 4), "unit": "GLUPS", "cores": cores,
                          "kind": "port",
                          "sample": f"{sweeps} update of the 512^3 field per step, NumPy oracle "

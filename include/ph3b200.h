@@ -121,6 +121,16 @@ int ph3_tb2d(const void* u, void* out, const float* src, int ny, int nx, int k, 
              float c1, int storage, int bc, int chunk, void* stream);
 
 /*
+ * Geometry of the pass ph3_tb2d / ph3_tb3d make on this grid (the tuning table applied; 16-byte
+ * aligned buffers assumed): the extended tile of one work item, *tx columns by *ty rows (*ty = 1
+ * in 2D), and its chunk *chunk (planes in 3D, rows in 2D). Launches nothing; needs a device.
+ * These are the inputs of pyheat3d's halo-traffic model of overlapped tiling, which
+ * src/pyheat3d/benchmark.py:219-230 reads from the CuPy stepper's `tile` (traffic.py:38-50).
+ */
+int ph3_tb_tile(int dims, int nz, int ny, int nx, int storage, int bc, int k, int* tx, int* ty,
+                int* chunk);
+
+/*
  * Advance `nsteps` time steps / Jacobi sweeps on the ping-pong pair (a, b), starting from the
  * state in `a`: nsteps / k passes of the variant's main kernel, then nsteps % k single steps
  * (cupy_backend.py:188-194). *in_b is set to 1 when the final state is in `b`, else 0.
@@ -195,7 +205,8 @@ int ph3_batch_launch(void* ws, int n, void* stream);
  * PH3_EINVAL. Every call shares the array: the counters are cleared and the plan rewritten on
  * each call, and calls that overlap on the GPU race, so the caller must serialise them. The
  * first call on a device looks up the array's device address (make it before any stream
- * capture); each call synchronises `stream` after uploading the plan. Results equal
+ * capture); each call synchronises `stream` after uploading the plan. The array used is the
+ * current device's, so `stream` must belong to the current device. Results equal
  * ph3_batch_prepare + ph3_batch_launch bit for bit.
  */
 int ph3_batch_run_static(const ph3_problem* problems, int n, void* stream);

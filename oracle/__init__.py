@@ -18,6 +18,7 @@ from .stencil import (  # noqa: F401
     reference_step,
     round_storage,
     run_reference,
+    threaded_emulated,
     threaded_step,
     to_bf16_bits,
 )

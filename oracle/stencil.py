@@ -199,3 +199,38 @@ def threaded_step(u: np.ndarray, out: np.ndarray, c0: float, c1: float, bc: str,
             _slab_update(u, out, c0, c1, periodic, b, a, e)
         return
     list(pool.map(lambda ae: _slab_update(u, out, c0, c1, periodic, b, *ae), jobs))
+
+
+def threaded_emulated(u0: np.ndarray, c0: float, c1: float, bc: str, steps: int,
+                      storage: str = "float32", k: int = 1, b: np.ndarray | None = None,
+                      threads: int | None = None, snapshots: tuple[int, ...] = ()
+                      ) -> np.ndarray | dict[int, np.ndarray]:
+    """:func:`emulated_reference` computed with :func:`threaded_step` (bit-identical result).
+
+    For full-size grids: every update runs thread-chunked over slabs of axis 0, and the storage
+    rounding follows the same schedule (after every pass of ``k`` updates, then after every
+    leftover single update). With ``snapshots`` (step counts), returns ``{step: state}`` for
+    each requested step reached on the way to ``steps`` (fp32 only, ``k`` = 1), so one
+    trajectory serves several checks.
+    """
+    threads = max(1, threads or os.cpu_count() or 1)
+    u = round_storage(np.array(u0, dtype=np.float32, copy=True), storage)
+    out = u.copy()  # carries the Dirichlet boundary values
+    passes, rem = divmod(steps, k)
+    schedule = [k] * passes + [1] * rem
+    want = set(snapshots)
+    snaps: dict[int, np.ndarray] = {}
+    done = 0
+    with ThreadPoolExecutor(threads) as pool:
+        for n in schedule:
+            for _ in range(n):
+                threaded_step(u, out, c0, c1, bc, b, threads=threads, pool=pool)
+                u, out = out, u
+                done += 1
+                if done in want:
+                    snaps[done] = u.copy()
+            if storage != "float32":
+                u[...] = round_storage(u, storage)
+    if want:
+        return snaps
+    return u

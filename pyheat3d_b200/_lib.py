@@ -30,6 +30,8 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "ph3_ymarch2d": (_i, [_p, _p, _p, _i, _i, _f, _f, _i, _i, _i, _p]),
     "ph3_tb3d": (_i, [_p, _p, _p, _i, _i, _i, _i, _f, _f, _i, _i, _i, _p]),
     "ph3_tb2d": (_i, [_p, _p, _p, _i, _i, _i, _f, _f, _i, _i, _i, _p]),
+    "ph3_tb_tile": (_i, [_i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(_i), ctypes.POINTER(_i),
+                         ctypes.POINTER(_i)]),
     "ph3_advance": (_i, [_i, _i, _i, _i, _i, _i, _f, _f, _i, _i, _p, _p, _p, _i64, _p,
                          ctypes.POINTER(_i)]),
     "ph3_reduction_scratch_len": (_i64, []),
@@ -47,6 +49,9 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "ph3_tune_set": (_i, [_i, _i, _i, _i, _i, _i]),
     "ph3_tune_get": (_i, [_i, _i, _i, _i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
 }
+
+#: size of the fixed device workspace behind ph3_batch_run_static (include/ph3b200.h)
+STATIC_BATCH_BYTES = 1 << 20
 
 #: tuning-table kernel families (include/ph3b200.h PH3_KERNEL_*)
 KERNEL = {"zmarch": 0, "march": 1, "tb": 2, "naive": 3, "batch": 4}

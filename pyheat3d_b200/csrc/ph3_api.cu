@@ -116,6 +116,7 @@ Launch make(int dims, int nz, int ny, int nx, int storage, int bc, float c0, flo
     L.zb = 0; L.ze = 0;
     L.stream = static_cast<cudaStream_t>(stream);
     L.err = status_ptr();
+    L.geo = nullptr;
     return L;
 }
 
@@ -143,15 +144,16 @@ cudaError_t launch_tb_tuned(Launch L) {
 }  // namespace
 
 int sm_count() {
-    static int counts[kMaxDev] = {0};
+    // concurrent first calls may both query the device; they store the same value atomically
+    static std::atomic<int> counts[kMaxDev];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return 0;
-    if (counts[dev] == 0) {
-        int n = 0;
+    int n = counts[dev].load(std::memory_order_acquire);
+    if (n == 0) {
         if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-        counts[dev] = n;
+        counts[dev].store(n, std::memory_order_release);
     }
-    return counts[dev];
+    return n;
 }
 
 }  // namespace ph3
@@ -283,6 +285,26 @@ int ph3_tb3d(const void* u, void* out, const float* src, int nz, int ny, int nx,
 int ph3_tb2d(const void* u, void* out, const float* src, int ny, int nx, int k, float c0,
              float c1, int storage, int bc, int chunk, void* stream) {
     return tb_common(2, u, out, src, 1, ny, nx, k, c0, c1, storage, bc, chunk, stream);
+}
+
+int ph3_tb_tile(int dims, int nz, int ny, int nx, int storage, int bc, int k, int* tx, int* ty,
+                int* chunk) {
+    int rc = check_grid(dims, dims == 2 ? 1 : nz, ny, nx, storage, bc);
+    if (rc != PH3_OK) return rc;
+    if (k != 2 && k != 3 && k != 4 && k != 8)
+        return fail(PH3_EINVAL, "tb k must be one of 2, 3, 4, 8, got %d", k);
+    if (tx == nullptr || ty == nullptr || chunk == nullptr)
+        return fail(PH3_EINVAL, "tx, ty and chunk must be non-null");
+    int geo[3] = {0, 0, 0};
+    Launch L = make(dims, nz, ny, nx, storage, bc, 0.f, 0.f, nullptr, nullptr, nullptr, k, 0,
+                    nullptr);
+    L.geo = geo;
+    rc = finish(launch_tb_tuned(L), "tb geometry");
+    if (rc != PH3_OK) return rc;
+    *tx = geo[0];
+    *ty = geo[1];
+    *chunk = geo[2];
+    return PH3_OK;
 }
 
 int ph3_advance(int dims, int nz, int ny, int nx, int storage, int bc, float c0, float c1,

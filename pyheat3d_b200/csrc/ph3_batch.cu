@@ -18,9 +18,12 @@
 // item number with two binary searches.
 //
 // Workspace layout (caller-allocated device memory, ph3_batch_workspace_bytes):
-//   [counters: u64 next item | i32 abort | i32 pad | i32 done[n]]  (rounded up to 256 bytes)
+//   [counters: u64 next item | i32 abort | i32 pad | u64 done[n]]  (rounded up to 256 bytes)
 //   [header][descriptors][order (i32)][tile prefix (i64)][round offsets (i64)]
+// The per-problem done counters are 64-bit: a problem counts steps x tiles completions, which
+// exceeds 2^31 for a large grid run for many steps.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -77,7 +80,7 @@ Geo geo_of(int cfg) {
 constexpr int kThreads = 32 * kW;
 
 __host__ __device__ __forceinline__ long long counter_bytes(int n) {
-    return ((16LL + 4LL * n + 255) / 256) * 256;
+    return ((16LL + 8LL * n + 255) / 256) * 256;
 }
 long long align256(long long x) { return ((x + 255) / 256) * 256; }
 
@@ -130,7 +133,7 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
     __shared__ long long s_item;
     unsigned long long* next = reinterpret_cast<unsigned long long*>(ws);
     int* abort_flag = reinterpret_cast<int*>(ws + 8);
-    int* done = reinterpret_cast<int*>(ws + 16);
+    unsigned long long* done = reinterpret_cast<unsigned long long*>(ws + 16);
     const BatchHeader* hd = reinterpret_cast<const BatchHeader*>(ws + counter_bytes(n));
     const unsigned char* base = reinterpret_cast<const unsigned char*>(hd);
     const BatchDesc* desc = reinterpret_cast<const BatchDesc*>(base + hd->off_desc);
@@ -154,8 +157,9 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
                 s_p = p;
                 s_s = s;
                 s_t = int(j - tilepre[q]);
-                const int need = s * desc[p].ntiles;
-                if (!wait_flag_geq(&done[p], need, kSpinLimit, err, abort_flag)) {
+                const unsigned long long need =
+                    static_cast<unsigned long long>(s) * static_cast<unsigned long long>(desc[p].ntiles);
+                if (!wait_u64_geq(&done[p], need, kSpinLimit, err, abort_flag)) {
                     atomicExch(abort_flag, 1);
                     item = -1;
                 }
@@ -175,24 +179,25 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
-            atomicAdd(&done[s_p], 1);
+            atomicAdd(&done[s_p], 1ULL);
         }
     }
 }
 
 int blocks_per_sm_cached() {
-    static int nb[64] = {0};
+    // per device; concurrent first calls may both query, and store the same value atomically
+    static std::atomic<int> nb[64];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
-    if (nb[dev] == 0) {
-        int v = 0;
+    int v = nb[dev].load(std::memory_order_acquire);
+    if (v == 0) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, batch_kernel, kThreads, 0) !=
                 cudaSuccess ||
             v < 1)
             v = 1;
-        nb[dev] = v;
+        nb[dev].store(v, std::memory_order_release);
     }
-    return nb[dev];
+    return v;
 }
 
 int cdiv(long long a, long long b) { return int((a + b - 1) / b); }
@@ -313,8 +318,10 @@ std::mutex g_static_mu;                          // serialises the host-side pla
 unsigned char g_static_img[kStaticWsBytes];      // host staging of the plan (no heap use)
 
 // Device address of g_static_ws on the current device, looked up once per device.
+// Concurrent first calls on one device may both look it up; they store the same address
+// atomically.
 unsigned char* static_ws_device(cudaError_t* err) {
-    static unsigned char* ptrs[64] = {nullptr};
+    static std::atomic<unsigned char*> ptrs[64];
     int dev = 0;
     *err = cudaGetDevice(&dev);
     if (*err != cudaSuccess) return nullptr;
@@ -322,13 +329,15 @@ unsigned char* static_ws_device(cudaError_t* err) {
         *err = cudaErrorInvalidDevice;
         return nullptr;
     }
-    if (ptrs[dev] == nullptr) {
+    unsigned char* ptr = ptrs[dev].load(std::memory_order_acquire);
+    if (ptr == nullptr) {
         void* p = nullptr;
         *err = cudaGetSymbolAddress(&p, g_static_ws);
         if (*err != cudaSuccess) return nullptr;
-        ptrs[dev] = static_cast<unsigned char*>(p);
+        ptr = static_cast<unsigned char*>(p);
+        ptrs[dev].store(ptr, std::memory_order_release);
     }
-    return ptrs[dev];
+    return ptr;
 }
 
 }  // namespace

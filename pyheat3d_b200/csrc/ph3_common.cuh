@@ -272,6 +272,28 @@ __device__ __forceinline__ bool wait_flag_geq(const int* flag, int target, uint3
     return true;
 }
 
+__device__ __forceinline__ unsigned long long ld_acquire_gpu_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// wait_flag_geq for a 64-bit counter.
+__device__ __forceinline__ bool wait_u64_geq(const unsigned long long* flag,
+                                             unsigned long long target, uint32_t limit, int* err,
+                                             const int* abort) {
+    uint32_t spins = 0;
+    while (ld_acquire_gpu_u64(flag) < target) {
+        __nanosleep(spins < 64 ? 32 : 256);
+        if (++spins > limit ||
+            (abort != nullptr && *reinterpret_cast<const volatile int*>(abort) != 0)) {
+            record_error(err, kDevDependTimeout);
+            return false;
+        }
+    }
+    return true;
+}
+
 // ------------------------------------------------------------------------------------------
 // mbarrier + TMA (cp.async.bulk) wrappers, written from the PTX ISA
 // ------------------------------------------------------------------------------------------

@@ -27,6 +27,8 @@ struct Launch {
                         // 1 <= zb <= ze <= nz-1); ze == 0: every plane the boundary allows
     cudaStream_t stream;
     int* err;           // device status word for bounded waits (may be null)
+    int* geo;           // tb<k> only: when set, the launcher writes the extended tile width,
+                        // height (1 in 2D) and chunk of its work items here and launches nothing
 };
 
 // Kernel families (ph3_stencil.cu, ph3_zmarch.cu). Each returns the launch status.
@@ -41,6 +43,9 @@ bool ring3d_supported(const Launch& L);
 cudaError_t launch_tbbulk(const Launch& L);     // 3D tb with a bulk-copy ring, aligned shapes
 bool tbbulk_supported(const Launch& L);
 int tbbulk_configs(int k, const char** names, int max);
+cudaError_t launch_tb2d(const Launch& L);       // 2D tb, two-row wavefront (any shape)
+int tb2d_configs(int k, const char** names, int max);
+cudaError_t launch_tb3d_planes(const Launch& L);  // 3D tb, shared-memory level planes (any shape)
 
 // Kernel families with selectable compiled configurations (the tuning table's first index).
 enum Family : int {

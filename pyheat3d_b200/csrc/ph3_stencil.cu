@@ -1,8 +1,9 @@
-// Stencil kernels for any grid shape (sm_100a): naive single-site kernels, register marches
-// for one time step, and temporal-blocking (tb<k>) wavefront kernels.
+// Stencil kernels for any grid shape (sm_100a): naive single-site kernels and register marches
+// for one time step; the dispatch of the temporal-blocking (tb<k>) families, whose kernels live
+// in ph3_tb2d.cu (2D), ph3_tbbulk.cu (3D, aligned rows) and ph3_tbsmem.cu (3D, any rows).
 //
 // Functional spec (what, not how): pyheat3d src/pyheat3d/backends/stencil.cu
-//   naive2d/naive3d :43-93, zmarch3d :101-161, tb3d :178-281, tb2d (K=1 -> ymarch) :289-385,
+//   naive2d/naive3d :43-93, zmarch3d :101-161, tb2d with K = 1 (the y-march) :289-385,
 // with the launch/remainder semantics of src/pyheat3d/backends/cupy_backend.py:141-194.
 //
 // Layout: C order, (z, y, x) / (y, x), x contiguous; storage fp32, fp16 or bf16; fp32 math.
@@ -91,230 +92,6 @@ march3d_k1_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __res
     __shared__ __align__(16) float edge[2 * W * 32 * V];
     march3d_item<T, PER, V, R, W, false>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x, blockIdx.y,
                                          blockIdx.z, zch, vec_i != 0, edge);
-}
-
-// ------------------------------------------------------------------------------------------
-// temporal blocking, 3D: k fused steps per pass, (z, t) wavefront with overlapped tiling.
-// The block's extended xy tile is 32*V x W*R sites (lane l: V columns, warp w: R rows); the
-// valid region shrinks by one site per level and only the centre OX x OY sites are stored.
-// Level s (1..K) of plane iz-s is computed while plane iz+1 is in flight; each level keeps a
-// 3-plane register queue. The x halo is rounded up to whole vectors so loads and stores stay
-// aligned vectors.
-// ------------------------------------------------------------------------------------------
-template <typename T, bool PER, int K, int V, int R, int W>
-__global__ void __launch_bounds__(32 * W)
-tb3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
-            int ny, int nx, float c0, float c1, int zch, int vec_i) {
-    constexpr int KX = ((K + V - 1) / V) * V;
-    constexpr int EX = 32 * V, OX = EX - 2 * KX;
-    constexpr int EY = W * R, OY = EY - 2 * K;
-    static_assert(OX > 0 && OY > 0, "tile too small for k");
-    __shared__ __align__(16) float edge[2][2][W][EX];  // [buffer][first/last][warp][column]
-    const bool vec = vec_i != 0;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int gx = blockIdx.x * OX - KX + lane * V;
-    const int gy0 = blockIdx.y * OY - K + w * R;
-    const int z0 = blockIdx.z * zch, z1 = min(z0 + zch, nz);
-    const int64_t P = int64_t(nx) * ny;
-
-    Cols<PER, V> cols;
-    cols.init(gx, nx, vec);
-    int64_t roff[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) roff[r] = int64_t(fix_near<PER>(gy0 + r, ny)) * nx;
-    uint32_t fixx = 0, fixy = 0;  // Dirichlet: boundary or outside sites keep their value
-    if constexpr (!PER) {
-#pragma unroll
-        for (int j = 0; j < V; ++j)
-            if (gx + j <= 0 || gx + j >= nx - 1) fixx |= 1u << j;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (gy0 + r <= 0 || gy0 + r >= ny - 1) fixy |= 1u << r;
-    }
-    const int lx = lane * V;
-    const bool xwriter = lx >= KX && lx < KX + OX;
-
-    float q[K][3][R][V];
-#pragma unroll
-    for (int s = 0; s < K; ++s)
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int j = 0; j < V; ++j) q[s][a][r][j] = 0.f;
-
-    float pre[R][V];
-    auto load_plane = [&](int z, float (&dst)[R][V]) {
-        const T* pl = u + int64_t(fix_near<PER>(z, nz)) * P;
-#pragma unroll
-        for (int r = 0; r < R; ++r) cols.load(pl + roff[r], vec, dst[r]);
-    };
-    load_plane(z0 - K, pre);
-    int buf = 0;
-
-    for (int iz = z0 - K; iz < z1 + K; ++iz) {
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-                q[0][0][r][j] = q[0][1][r][j];
-                q[0][1][r][j] = q[0][2][r][j];
-                q[0][2][r][j] = pre[r][j];
-            }
-        if (iz + 1 < z1 + K) load_plane(iz + 1, pre);
-        float res[R][V];
-#pragma unroll
-        for (int s = 1; s <= K; ++s) {
-            const int c = iz - s;
-            float up[V], dn[V];
-            if constexpr (W > 1) {
-#pragma unroll
-                for (int j = 0; j < V; ++j) {
-                    edge[buf][0][w][lx + j] = q[s - 1][1][0][j];
-                    edge[buf][1][w][lx + j] = q[s - 1][1][R - 1][j];
-                }
-                __syncthreads();
-#pragma unroll
-                for (int j = 0; j < V; ++j) {
-                    up[j] = w > 0 ? edge[buf][1][w - 1][lx + j] : q[s - 1][1][0][j];
-                    dn[j] = w < W - 1 ? edge[buf][0][w + 1][lx + j] : q[s - 1][1][R - 1][j];
-                }
-                buf ^= 1;
-            } else {
-#pragma unroll
-                for (int j = 0; j < V; ++j) { up[j] = q[s - 1][1][0][j]; dn[j] = q[s - 1][1][R - 1][j]; }
-            }
-            const bool zfix = !PER && (c <= 0 || c >= nz - 1);
-            const float* bpl = b != nullptr ? b + int64_t(fix_near<PER>(c, nz)) * P : nullptr;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const float left = __shfl_up_sync(kFull, q[s - 1][1][r][V - 1], 1);
-                const float right = __shfl_down_sync(kFull, q[s - 1][1][r][0], 1);
-                float bv[V];
-                if (bpl != nullptr) cols.load_src(bpl + roff[r], vec, bv);
-#pragma unroll
-                for (int j = 0; j < V; ++j) {
-                    const float ctr = q[s - 1][1][r][j];
-                    const float xm = j > 0 ? q[s - 1][1][r][j - 1] : left;
-                    const float xp = j < V - 1 ? q[s - 1][1][r][j + 1] : right;
-                    const float ym = r > 0 ? q[s - 1][1][r - 1][j] : up[j];
-                    const float yp = r < R - 1 ? q[s - 1][1][r + 1][j] : dn[j];
-                    float v = upd3(c0, c1, ctr, xm, xp, ym, yp, q[s - 1][0][r][j], q[s - 1][2][r][j]);
-                    if (bpl != nullptr) v = __fadd_rn(v, bv[j]);
-                    if constexpr (!PER) {
-                        if (zfix || ((fixy >> r) & 1u) || ((fixx >> j) & 1u)) v = ctr;
-                    }
-                    res[r][j] = v;
-                }
-            }
-            if (s < K) {
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-#pragma unroll
-                    for (int j = 0; j < V; ++j) {
-                        q[s][0][r][j] = q[s][1][r][j];
-                        q[s][1][r][j] = q[s][2][r][j];
-                        q[s][2][r][j] = res[r][j];
-                    }
-            }
-        }
-        const int c = iz - K;
-        const bool zok = c >= z0 && c < z1 && (PER || (c > 0 && c < nz - 1));
-        if (zok && xwriter) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int row = w * R + r, gy = gy0 + r;
-                if (row >= K && row < K + OY && gy < ny && !((fixy >> r) & 1u))
-                    store_cols<T, V>(o + int64_t(c) * P + int64_t(gy) * nx, gx, nx, vec, fixx,
-                                     res[r]);
-            }
-        }
-    }
-}
-
-// ------------------------------------------------------------------------------------------
-// temporal blocking, 2D: warp-synchronous; each warp owns an extended strip of 32*V columns
-// and walks a chunk of rows with a K-level 3-row register queue. No shared memory, no block
-// sync. Strips overlap by 2*KX columns.
-// ------------------------------------------------------------------------------------------
-template <typename T, bool PER, int K, int V, int W>
-__global__ void __launch_bounds__(32 * W)
-tb2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int ny,
-            int nx, float c0, float c1, int ych, int vec_i) {
-    constexpr int KX = ((K + V - 1) / V) * V;
-    constexpr int EX = 32 * V, OX = EX - 2 * KX;
-    static_assert(OX > 0, "strip too narrow for k");
-    const bool vec = vec_i != 0;
-    const int lane = threadIdx.x & 31;
-    const int strip = blockIdx.x * W + (threadIdx.x >> 5);
-    if (strip * OX >= nx) return;  // warp-uniform; no block sync in this kernel
-    const int gx = strip * OX - KX + lane * V;
-    const int y0 = blockIdx.y * ych, y1 = min(y0 + ych, ny);
-
-    Cols<PER, V> cols;
-    cols.init(gx, nx, vec);
-    uint32_t fixx = 0;
-    if constexpr (!PER) {
-#pragma unroll
-        for (int j = 0; j < V; ++j)
-            if (gx + j <= 0 || gx + j >= nx - 1) fixx |= 1u << j;
-    }
-    const int lx = lane * V;
-    const bool xwriter = lx >= KX && lx < KX + OX;
-
-    float q[K][3][V];
-#pragma unroll
-    for (int s = 0; s < K; ++s)
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int j = 0; j < V; ++j) q[s][a][j] = 0.f;
-    float pre[V];
-    cols.load(u + int64_t(fix_near<PER>(y0 - K, ny)) * nx, vec, pre);
-
-    for (int iy = y0 - K; iy < y1 + K; ++iy) {
-#pragma unroll
-        for (int j = 0; j < V; ++j) {
-            q[0][0][j] = q[0][1][j];
-            q[0][1][j] = q[0][2][j];
-            q[0][2][j] = pre[j];
-        }
-        if (iy + 1 < y1 + K) cols.load(u + int64_t(fix_near<PER>(iy + 1, ny)) * nx, vec, pre);
-        float res[V];
-#pragma unroll
-        for (int s = 1; s <= K; ++s) {
-            const int c = iy - s;
-            const bool yfix = !PER && (c <= 0 || c >= ny - 1);
-            const float left = __shfl_up_sync(kFull, q[s - 1][1][V - 1], 1);
-            const float right = __shfl_down_sync(kFull, q[s - 1][1][0], 1);
-            float bv[V];
-            if (b != nullptr) cols.load_src(b + int64_t(fix_near<PER>(c, ny)) * nx, vec, bv);
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-                const float ctr = q[s - 1][1][j];
-                const float xm = j > 0 ? q[s - 1][1][j - 1] : left;
-                const float xp = j < V - 1 ? q[s - 1][1][j + 1] : right;
-                float v = upd2(c0, c1, ctr, xm, xp, q[s - 1][0][j], q[s - 1][2][j]);
-                if (b != nullptr) v = __fadd_rn(v, bv[j]);
-                if constexpr (!PER) {
-                    if (yfix || ((fixx >> j) & 1u)) v = ctr;
-                }
-                res[j] = v;
-            }
-            if (s < K) {
-#pragma unroll
-                for (int j = 0; j < V; ++j) {
-                    q[s][0][j] = q[s][1][j];
-                    q[s][1][j] = q[s][2][j];
-                    q[s][2][j] = res[j];
-                }
-            }
-        }
-        const int c = iy - K;
-        const bool yok = c >= y0 && c < y1 && (PER || (c > 0 && c < ny - 1));
-        if (yok && xwriter) store_cols<T, V>(o + int64_t(c) * nx, gx, nx, vec, fixx, res);
-    }
 }
 
 template <typename T, bool PER, int R, int W>
@@ -489,55 +266,6 @@ static cudaError_t march_k1_t(const Launch& L) {
     return cudaGetLastError();
 }
 
-template <typename T, bool PER, int K, int V, int R, int W>
-static cudaError_t tb3d_t(const Launch& L) {
-    constexpr int KX = ((K + V - 1) / V) * V, OX = 32 * V - 2 * KX, OY = W * R - 2 * K;
-    const long long tiles = 1LL * cdiv(L.nx, OX) * cdiv(L.ny, OY);
-    const int zch = L.chunk > 0 ? L.chunk
-                                : default_chunk(L.nz, tiles, std::max(8, 4 * K), 4LL * sm_count());
-    dim3 grd(cdiv(L.nx, OX), cdiv(L.ny, OY), cdiv(L.nz, zch));
-    if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
-    tb3d_kernel<T, PER, K, V, R, W><<<grd, 32 * W, 0, L.stream>>>(
-        static_cast<const T*>(L.u), static_cast<T*>(L.out), L.src, L.nz, L.ny, L.nx, L.c0, L.c1,
-        zch, vec_ok<T, PER, V>(L) ? 1 : 0);
-    return cudaGetLastError();
-}
-
-template <typename T, bool PER, int K, int V, int W>
-static cudaError_t tb2d_t(const Launch& L) {
-    constexpr int KX = ((K + V - 1) / V) * V, OX = 32 * V - 2 * KX;
-    const int strips = cdiv(L.nx, OX);
-    const int ych = L.chunk > 0 ? L.chunk
-                                : default_chunk(L.ny, cdiv(strips, W), std::max(16, 8 * K),
-                                                8LL * sm_count());
-    dim3 grd(cdiv(strips, W), cdiv(L.ny, ych));
-    if (grd.y > 65535) return cudaErrorInvalidConfiguration;
-    tb2d_kernel<T, PER, K, V, W><<<grd, 32 * W, 0, L.stream>>>(
-        static_cast<const T*>(L.u), static_cast<T*>(L.out), L.src, L.ny, L.nx, L.c0, L.c1, ych,
-        vec_ok<T, PER, V>(L) ? 1 : 0);
-    return cudaGetLastError();
-}
-
-template <typename T, bool PER>
-static cudaError_t tb_t(const Launch& L) {
-    if (L.dims == 2) {
-        switch (L.k) {
-            case 2: return tb2d_t<T, PER, 2, 4, 4>(L);
-            case 3: return tb2d_t<T, PER, 3, 4, 4>(L);
-            case 4: return tb2d_t<T, PER, 4, 4, 4>(L);
-            case 8: return tb2d_t<T, PER, 8, 4, 4>(L);
-            default: return cudaErrorInvalidValue;
-        }
-    }
-    switch (L.k) {
-        case 2: return tb3d_t<T, PER, 2, 4, 2, 16>(L);
-        case 3: return tb3d_t<T, PER, 3, 4, 2, 16>(L);
-        case 4: return tb3d_t<T, PER, 4, 2, 2, 16>(L);
-        case 8: return tb3d_t<T, PER, 8, 2, 1, 32>(L);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
 #define PH3_DISPATCH(fn, L)                                                               \
     do {                                                                                  \
         switch ((L).storage) {                                                            \
@@ -553,11 +281,10 @@ static cudaError_t tb_t(const Launch& L) {
 cudaError_t launch_naive(const Launch& L) { PH3_DISPATCH(naive_t, L); }
 cudaError_t launch_march_k1(const Launch& L) { PH3_DISPATCH(march_k1_t, L); }
 
-static cudaError_t launch_tb_plain(const Launch& L) { PH3_DISPATCH(tb_t, L); }
-
 cudaError_t launch_tb(const Launch& L) {
-    if (L.dims == 3 && tbbulk_supported(L)) return launch_tbbulk(L);
-    return launch_tb_plain(L);
+    if (L.dims == 2) return launch_tb2d(L);
+    if (tbbulk_supported(L)) return launch_tbbulk(L);
+    return launch_tb3d_planes(L);
 }
 
 // 2D: 0 lean one-column-per-lane march, 1 float-window vector march, 2 / 3 / 4 raw-row vector
@@ -575,10 +302,7 @@ int march_configs(int dims, const char** names, int max) {
 }
 
 int tb_configs(int dims, int k, const char** names, int max) {
-    if (dims == 3) return tbbulk_configs(k, names, max);
-    if (k != 2 && k != 3 && k != 4 && k != 8) return 0;
-    if (names != nullptr && max > 0) names[0] = "V4_W4";
-    return 1;
+    return dims == 3 ? tbbulk_configs(k, names, max) : tb2d_configs(k, names, max);
 }
 
 }  // namespace ph3

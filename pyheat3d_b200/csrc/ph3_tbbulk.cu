@@ -26,6 +26,7 @@
 // Requirements (else the plain-load tb3d kernel runs): nx * sizeof(T) % 16 == 0, 16-byte aligned
 // buffers, nx >= 16 / sizeof(T).
 #include <algorithm>
+#include <atomic>
 
 #include "ph3_common.cuh"
 #include "ph3_internal.h"
@@ -355,11 +356,12 @@ template <typename T, bool PER, int K, int V, int R, int NWC, int STAGES>
 cudaError_t tbbulk_t(const Launch& L) {
     using C = TbCfg<T, K, V, R, NWC, STAGES>;
     auto kern = tb3d_bulk_kernel<T, PER, K, V, R, NWC, STAGES>;
-    static int blocks_per_sm[64] = {0};
+    static std::atomic<int> blocks_per_sm[64];  // per device; first calls may race harmlessly
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (blocks_per_sm[dev] == 0) {
+    int nbl = blocks_per_sm[dev].load(std::memory_order_acquire);
+    if (nbl == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              C::SMEM);
         if (e != cudaSuccess) return e;
@@ -367,18 +369,23 @@ cudaError_t tbbulk_t(const Launch& L) {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, C::THREADS, C::SMEM);
         if (e != cudaSuccess) return e;
         if (nb < 1) return cudaErrorInvalidConfiguration;
-        blocks_per_sm[dev] = nb;
+        nbl = nb;
+        blocks_per_sm[dev].store(nbl, std::memory_order_release);
     }
     TbGeom g;
     g.nz = L.nz; g.ny = L.ny; g.nx = L.nx;
     g.ntx = (L.nx + C::OX - 1) / C::OX;
     g.nty = (L.ny + C::OY - 1) / C::OY;
     const long long tiles = 1LL * g.ntx * g.nty;
-    const long long blocks = 1LL * sm_count() * blocks_per_sm[dev];
+    const long long blocks = 1LL * sm_count() * nbl;
     g.zch = L.chunk > 0 ? std::min(L.chunk, L.nz) : balanced_chunk(L.nz, tiles, blocks, K);
     g.nch = (L.nz + g.zch - 1) / g.zch;
     const long long items = tiles * g.nch;
     if (items > (1LL << 30)) return cudaErrorInvalidValue;
+    if (L.geo != nullptr) {
+        L.geo[0] = C::EX; L.geo[1] = C::EY; L.geo[2] = g.zch;
+        return cudaSuccess;
+    }
     g.nitems = int(items);
     const int grid = int(std::min(items, blocks));
     kern<<<grid, C::THREADS, C::SMEM, L.stream>>>(static_cast<const T*>(L.u),

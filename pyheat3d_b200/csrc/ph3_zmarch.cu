@@ -23,6 +23,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "ph3_common.cuh"
@@ -863,14 +864,14 @@ cudaError_t ring3d_t(const Launch& L) {
     using C = RgCfg<T, PER, R, STAGES>;
     constexpr int SMEM = W * C::WARPB;
     auto kern = ring3d_kernel<T, PER, R, W, STAGES>;
-    static bool attr_set[64] = {false};  // per device
+    static std::atomic<bool> attr_set[64];  // per device; first calls may race harmlessly
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (!attr_set[dev]) {
+    if (!attr_set[dev].load(std::memory_order_acquire)) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
         if (e != cudaSuccess) return e;
-        attr_set[dev] = true;
+        attr_set[dev].store(true, std::memory_order_release);
     }
     const uint64_t n = uint64_t(L.nz) * L.ny * L.nx;
     CUtensorMap tr, th;
@@ -905,18 +906,20 @@ cudaError_t zmarch_t(const Launch& L) {
         else return zmarch_tma_kernel<T, PER, TY, NWC, STAGES, PACKED>;
     };
     auto kern = pick();
-    static int blocks_per_sm[64] = {0};  // per device
+    static std::atomic<int> blocks_per_sm[64];  // per device; first calls may race harmlessly
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (blocks_per_sm[dev] == 0) {
+    int nbl = blocks_per_sm[dev].load(std::memory_order_acquire);
+    if (nbl == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              C::SMEM);
         if (e != cudaSuccess) return e;
         int nb = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, C::THREADS, C::SMEM);
         if (e != cudaSuccess) return e;
-        blocks_per_sm[dev] = std::max(1, nb);
+        nbl = std::max(1, nb);
+        blocks_per_sm[dev].store(nbl, std::memory_order_release);
     }
     CUtensorMap tb, tr, ts;
     if (!make_map<T>(&tb, L.u, L.nz, L.ny, L.nx, C::TX, TY) ||
@@ -935,7 +938,7 @@ cudaError_t zmarch_t(const Launch& L) {
     }
     if (g.nzi <= 0) return cudaSuccess;
     const long long tiles = 1LL * g.ntx * g.nty;
-    const long long resident = 1LL * sm_count() * blocks_per_sm[dev];
+    const long long resident = 1LL * sm_count() * nbl;
     int zch = L.chunk;
     if (zch <= 0) {
         // chunk-major items; one chunk of the field (read + write) kept around half of L2 so the
@@ -954,7 +957,7 @@ cudaError_t zmarch_t(const Launch& L) {
     const long long nitems = tiles * g.nchunks;
     if (nitems > (1LL << 30)) return cudaErrorInvalidValue;
     g.nitems = int(nitems);
-    const int grid = int(std::min<long long>(nitems, 1LL * sm_count() * blocks_per_sm[dev]));
+    const int grid = int(std::min<long long>(nitems, 1LL * sm_count() * nbl));
     kern<<<grid, C::THREADS, C::SMEM, L.stream>>>(tb, tr, ts, static_cast<T*>(L.out), L.src, g,
                                                   L.c0, L.c1, L.err);
     return cudaGetLastError();

@@ -191,16 +191,19 @@ class GpuExecutor:
             d.c0, d.c1 = float(np.float32(c0)), float(np.float32(c1))
             d.steps = int(c)
             d.reserved = 0
-        stream = self.torch.cuda.current_stream(self.device).cuda_stream
         addr = ctypes.addressof(descs)
-        rc = self.lib.ph3_batch_run_static(addr, n, stream)
-        if rc != 0:  # plan larger than the library's fixed workspace: use an allocated one
-            need = int(self.lib.ph3_batch_workspace_bytes(addr, n))
-            if self._ws is None or self._ws.numel() < need:
-                self._ws = self.torch.empty(need, dtype=self.torch.uint8, device=self.device)
-            _lib.check(self.lib.ph3_batch_prepare(addr, n, self._ws.data_ptr(), self._ws.numel(),
-                                                  stream))
-            _lib.check(self.lib.ph3_batch_launch(self._ws.data_ptr(), n, stream))
+        need = int(self.lib.ph3_batch_workspace_bytes(addr, n))
+        # the library's fixed workspace belongs to the current device: make it this one
+        with self.torch.cuda.device(self.device):
+            stream = self.torch.cuda.current_stream(self.device).cuda_stream
+            if need <= _lib.STATIC_BATCH_BYTES:
+                _lib.check(self.lib.ph3_batch_run_static(addr, n, stream))
+            else:  # plan larger than the fixed workspace: use an allocated one
+                if self._ws is None or self._ws.numel() < need:
+                    self._ws = self.torch.empty(need, dtype=self.torch.uint8, device=self.device)
+                _lib.check(self.lib.ph3_batch_prepare(addr, n, self._ws.data_ptr(),
+                                                      self._ws.numel(), stream))
+                _lib.check(self.lib.ph3_batch_launch(self._ws.data_ptr(), n, stream))
         for s, c in zip(slots, counts):
             if c % 2:
                 s.in_b = not s.in_b

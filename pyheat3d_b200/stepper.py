@@ -67,6 +67,13 @@ class B200Stepper(Stepper):
         self._variant = _lib.VARIANT[self.kind]
         self._k = self.K if self.kind == "tb" else 1
         self.tile = {"kind": self.kind, "k": self._k}
+        if self.kind == "tb":  # the tile of the tb<k> pass, for pyheat3d's halo-traffic model
+            configure(self.dims, self.storage, self._k, self.ncells, self._lib)
+            tx, ty, ch = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+            _lib.check(self._lib.ph3_tb_tile(
+                self.dims, self._nz, self._ny, self._nx, _lib.STORAGE[self.storage],
+                _lib.BC[self.bc], self._k, ctypes.byref(tx), ctypes.byref(ty), ctypes.byref(ch)))
+            self.tile.update({"tx": tx.value, "ty": ty.value, "zch": ch.value})
         self._in_b = ctypes.c_int(0)
 
     # -- stepping ------------------------------------------------------------------------

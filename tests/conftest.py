@@ -3,9 +3,10 @@
 ``gpu`` tests need a CUDA device and the built ``libph3b200.so``; without a device they are
 skipped (the reference's ``tests/conftest.py:6-12`` does the same).
 
-If a pyheat3d checkout sits next to this repository (``../reference/src``) or ``PYHEAT3D_SRC``
-names one, it is put on ``sys.path`` so the CPU tests can check the registry plug-in against the
-real pyheat3d. GPU tests never need it.
+If ``PYHEAT3D_SRC`` names a pyheat3d source tree (the directory holding the ``pyheat3d``
+package), or a pyheat3d checkout sits beside this repository (``<sibling>/src/pyheat3d``), it is
+put on ``sys.path`` so the CPU tests can check the registry plug-in against the real pyheat3d.
+GPU tests never need it.
 """
 
 from __future__ import annotations
@@ -20,12 +21,22 @@ ROOT = Path(__file__).resolve().parents[1]
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
-_cands = [os.environ.get("PYHEAT3D_SRC"), str(ROOT.parent / "reference" / "src")]
-for _c in _cands:
-    if _c and (Path(_c) / "pyheat3d" / "__init__.py").exists():
-        if _c not in sys.path:
-            sys.path.append(_c)
-        break
+def _pyheat3d_src() -> str | None:
+    env = os.environ.get("PYHEAT3D_SRC")
+    if env and (Path(env) / "pyheat3d" / "__init__.py").exists():
+        return env
+    try:
+        for sib in sorted(ROOT.parent.iterdir()):
+            if sib != ROOT and (sib / "src" / "pyheat3d" / "__init__.py").is_file():
+                return str(sib / "src")
+    except OSError:
+        pass
+    return None
+
+
+_src = _pyheat3d_src()
+if _src and _src not in sys.path:
+    sys.path.append(_src)
 
 
 def _cuda_ok() -> bool:

@@ -2,7 +2,7 @@
 
 Run in a checkout where the pyheat3d sources are importable, e.g.::
 
-    PYTHONPATH=/root/reference/src python tests/golden/make_golden.py
+    PYTHONPATH=<pyheat3d checkout>/src python tests/golden/make_golden.py
 
 It imports the reference's own ``reference_step`` (``src/pyheat3d/backends/numpy_ref.py:30``),
 ``emulated_reference`` / ``round_storage`` (``src/pyheat3d/validation.py:157-183``),

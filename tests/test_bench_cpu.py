@@ -41,7 +41,9 @@ def test_reference_arm_prints_one_contract_line():
     finally:
         sys.path.remove(str(ROOT))
     # the same workload description as the B200 arm (one update per bench step here)
-    assert d["config"] == bench.workload_config(3, 512, "float32", 1, 1)
+    # the same config object as the GPU arm's line; the per-step work is a separate key
+    assert d["config"] == bench.workload_config(3, 512, "float32", 1)
+    assert d["time_steps_per_step"] == 1
 
 
 def test_reference_arm_other_ranks_exit_quietly():

@@ -20,6 +20,7 @@ from oracle import (
     reference_step,
     round_storage,
     run_reference,
+    threaded_emulated,
     threaded_step,
     to_bf16_bits,
 )
@@ -131,3 +132,24 @@ def test_dirichlet128_hash_matches_reference_run():
             threaded_step(u, out, cfg["c0"], cfg["c1"], "dirichlet", threads=8, pool=pool)
             u, out = out, u
     assert hashlib.sha256(np.ascontiguousarray(u).tobytes()).hexdigest() == cfg["sha256"]
+
+
+@pytest.mark.parametrize("storage,k,bc", [("float32", 1, "periodic"), ("bfloat16", 4, "periodic"),
+                                          ("float16", 3, "dirichlet"), ("bfloat16", 1, "dirichlet"),
+                                          ("float16", 8, "periodic")])
+@pytest.mark.parametrize("dims", [2, 3])
+def test_threaded_emulated_is_bitwise_emulated_reference(dims, storage, k, bc):
+    """The full-size GPU tests check 16-bit and tb<k> variants against this threaded form."""
+    shape = (13, 17, 19) if dims == 3 else (37, 41)
+    u0 = np.random.default_rng(2).random(shape, dtype=np.float32)
+    c0, c1 = heat(dims, bc)
+    got = threaded_emulated(u0, c0, c1, bc, 2 * k + 1, storage, k, threads=4)
+    assert np.array_equal(got, emulated_reference(u0, c0, c1, bc, 2 * k + 1, storage, k))
+
+
+def test_threaded_emulated_snapshots():
+    u0 = np.random.default_rng(3).random((29, 31), dtype=np.float32)
+    c0, c1 = heat(2, "periodic")
+    snaps = threaded_emulated(u0, c0, c1, "periodic", 9, snapshots=(3, 5, 9), threads=3)
+    for n in (3, 5, 9):
+        assert np.array_equal(snaps[n], run_reference(u0, c0, c1, "periodic", n))
