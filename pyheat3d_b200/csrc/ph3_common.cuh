@@ -145,6 +145,33 @@ template <> struct Pack16<__half> {
     }
 };
 
+// One lane's LB bytes of storage <-> float2 pairs: LB = 16 is Pack16; LB = 8 holds 2 fp32 or
+// 4 16-bit values.
+template <typename T, int LB> struct PackLane;
+template <typename T> struct PackLane<T, 16> : Pack16<T> { using W = uint4; };
+template <> struct PackLane<float, 8> {
+    using W = uint2;
+    static constexpr int NP = 1;
+    __device__ __forceinline__ static void unpack(const uint2& w, float2 (&v)[NP]) {
+        v[0] = make_float2(__uint_as_float(w.x), __uint_as_float(w.y));
+    }
+    __device__ __forceinline__ static uint2 pack(const float2 (&v)[NP]) {
+        return make_uint2(__float_as_uint(v[0].x), __float_as_uint(v[0].y));
+    }
+};
+template <typename T> struct PackLane16x4 {
+    using W = uint2;
+    static constexpr int NP = 2;
+    __device__ __forceinline__ static void unpack(const uint2& w, float2 (&v)[NP]) {
+        v[0] = Pack16<T>::cvt(w.x); v[1] = Pack16<T>::cvt(w.y);
+    }
+    __device__ __forceinline__ static uint2 pack(const float2 (&v)[NP]) {
+        return make_uint2(Pack16<T>::rnd(v[0]), Pack16<T>::rnd(v[1]));
+    }
+};
+template <> struct PackLane<__nv_bfloat16, 8> : PackLane16x4<__nv_bfloat16> {};
+template <> struct PackLane<__half, 8> : PackLane16x4<__half> {};
+
 // ------------------------------------------------------------------------------------------
 // canonical-order stencil arithmetic
 // ------------------------------------------------------------------------------------------

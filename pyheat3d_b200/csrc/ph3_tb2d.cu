@@ -96,7 +96,7 @@ __device__ __forceinline__ void lds_pairs(const T* p, float2 (&v)[V / 2]) {
     for (int q = 0; q < V / 2; ++q) v[q] = make_float2(f[2 * q], f[2 * q + 1]);
 }
 
-template <typename T, bool PER, bool BULK, int K, int V, int STAGES, int W, int MINB>
+template <typename T, bool PER, bool SRC, bool BULK, int K, int V, int STAGES, int W, int MINB>
 __global__ void __launch_bounds__(32 * W, MINB)
 tb2d_pair_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b,
                  T2Geom g, float c0, float c1, int* err) {
@@ -220,7 +220,7 @@ tb2d_pair_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
         float2 sx[NP];
         xsum_row<NP>(ctr, sx);
         float2 bv[NP];
-        if (b != nullptr) {  // Jacobi source, added last
+        if constexpr (SRC) {  // Jacobi source, added last
             const float* brow = b + int64_t(row_of(c)) * g.nx;
             float f[V];
             if (bvec) {
@@ -238,7 +238,7 @@ tb2d_pair_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __rest
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
             float2 v = lin2(c0v, c1v, ctr[p], add2(sx[p], add2(ym[p], yp[p])));
-            if (b != nullptr) v = add2(v, bv[p]);
+            if constexpr (SRC) v = add2(v, bv[p]);
             if constexpr (!PER) {
                 if (rowfix || ((fixx >> (2 * p)) & 1u)) v.x = ctr[p].x;
                 if (rowfix || ((fixx >> (2 * p + 1)) & 1u)) v.y = ctr[p].y;
@@ -353,10 +353,10 @@ int t2_chunk(int ny, int nstrips, long long slots, int k) {
     return best;
 }
 
-template <typename T, bool PER, bool BULK, int K, int V, int STAGES, int W, int MINB>
+template <typename T, bool PER, bool SRC, bool BULK, int K, int V, int STAGES, int W, int MINB>
 cudaError_t t2_launch(const Launch& L) {
     using C = T2Cfg<T, K, V, STAGES>;
-    auto kern = tb2d_pair_kernel<T, PER, BULK, K, V, STAGES, W, MINB>;
+    auto kern = tb2d_pair_kernel<T, PER, SRC, BULK, K, V, STAGES, W, MINB>;
     constexpr int SMEM = BULK ? W * (C::RING_BYTES + STAGES * 8) : 0;
     static std::atomic<int> blocks_per_sm[64];  // per device; first calls may race harmlessly
     int dev = 0;
@@ -405,21 +405,27 @@ bool t2_bulk_ok(const Launch& L) {
            al(L.u) && al(L.out) && al(L.src);
 }
 
+// The Jacobi source is a compile-time choice: the kernel without it carries neither its loads
+// nor the branches around them (the loop body stays small enough for the instruction cache).
 template <typename T, bool PER, int K, int V, int STAGES, int W, int MINB>
 cudaError_t t2_pick(const Launch& L) {
-    if (t2_bulk_ok<T, V>(L)) return t2_launch<T, PER, true, K, V, STAGES, W, MINB>(L);
-    return t2_launch<T, PER, false, K, V, STAGES, W, MINB>(L);
+    const bool bulk = t2_bulk_ok<T, V>(L);
+    if (L.src != nullptr)
+        return bulk ? t2_launch<T, PER, true, true, K, V, STAGES, W, MINB>(L)
+                    : t2_launch<T, PER, true, false, K, V, STAGES, W, MINB>(L);
+    return bulk ? t2_launch<T, PER, false, true, K, V, STAGES, W, MINB>(L)
+                : t2_launch<T, PER, false, false, K, V, STAGES, W, MINB>(L);
 }
 
 // Compiled configurations per k: values per lane (EX = 32 V) and the register budget of a
-// thread (128: 16 resident warps per SM; 168: 12). 0 is the default for k <= 3, 1 for k >= 4,
-// where the kept row pairs of the levels need more registers.
+// thread (128: 16 resident warps per SM; 168: 12). 0 is the default for k <= 4, 1 for k = 8,
+// where the kept row pairs of the eight levels need more than 128 registers.
 constexpr int kT2Cfgs = 3;
 const char* kT2Names[kT2Cfgs] = {"pair_V4_R128", "pair_V4_R168", "pair_V2_R128"};
 
 template <typename T, bool PER, int K, int STAGES>
 cudaError_t t2_cfg(const Launch& L) {
-    const int cfg = L.cfg < 0 ? (K >= 4 ? 1 : 0) : L.cfg;
+    const int cfg = L.cfg < 0 ? (K >= 8 ? 1 : 0) : L.cfg;
     switch (cfg) {
         case 1: return t2_pick<T, PER, K, 4, STAGES, 4, 3>(L);
         case 2: return t2_pick<T, PER, K, 2, STAGES, 4, 4>(L);

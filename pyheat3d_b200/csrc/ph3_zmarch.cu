@@ -36,11 +36,11 @@ namespace {
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
-template <typename T, int TY, int NWC, int STAGES>
+template <typename T, int TY, int NWC, int STAGES, int LB = 16>
 struct ZmCfg {
-    static constexpr int V = 16 / int(sizeof(T));  // values per lane (one 16-byte vector)
-    static constexpr int TX = 32 * V;              // tile width: 512 bytes per row
-    static constexpr int HX = V;                   // halo column box: 16 bytes
+    static constexpr int V = LB / int(sizeof(T));  // values per lane (one LB-byte vector)
+    static constexpr int TX = 32 * V;              // tile width: 32 * LB bytes per row
+    static constexpr int HX = 16 / int(sizeof(T)); // halo column box: 16 bytes
     static constexpr int RW = TY / NWC;            // rows per consumer warp
     static_assert(TY % NWC == 0, "rows must split evenly over the consumer warps");
     static constexpr int BODY_BYTES = (TY + 2) * TX * int(sizeof(T));
@@ -78,9 +78,10 @@ struct SrcRows {
 };
 
 // Blocks per SM the register budget is sized for (the ring's shared memory allows as many).
-template <typename T, int TY, int NWC>
+template <typename T, int TY, int NWC, int LB = 16>
 constexpr int zm_min_blocks() {
     constexpr int RW = TY / NWC;
+    if (LB == 8) return 2;  // 4 values per lane: half the registers of a 16-byte lane
     if (NWC >= 16) return sizeof(T) == 4 ? 2 : 1;
     if (sizeof(T) == 4) return RW >= 4 ? 2 : 3;
     return RW >= 2 ? 1 : 3;
@@ -89,12 +90,12 @@ constexpr int zm_min_blocks() {
 // Producer (one thread): streams the planes zlo-1 .. zhi of every item of this block into the
 // ring, in the order the consumers take them. Stage s of plane number `it` is reused once all
 // NWC consumer warps released its previous use (the empty barrier's phase).
-template <typename T, bool PER, int TY, int NWC, int STAGES>
+template <typename T, bool PER, int TY, int NWC, int STAGES, int LB = 16>
 __device__ __forceinline__ void zm_produce(const CUtensorMap* tm_body, const CUtensorMap* tm_row,
                                            const CUtensorMap* tm_side, const ZmGeom& g,
                                            unsigned char* smem, uint64_t* full, uint64_t* empty,
                                            volatile int* issued, int* err) {
-    using C = ZmCfg<T, TY, NWC, STAGES>;
+    using C = ZmCfg<T, TY, NWC, STAGES, LB>;
     constexpr int TX = C::TX, HX = C::HX;
     prefetch_tmap(tm_body);
     prefetch_tmap(tm_row);
@@ -132,13 +133,14 @@ __device__ __forceinline__ void zm_produce(const CUtensorMap* tm_body, const CUt
     }
 }
 
-template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED>
-__global__ void __launch_bounds__(32 * (NWC + 1), zm_min_blocks<T, TY, NWC>())
+template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED, int LB = 16,
+          bool SRC = true>
+__global__ void __launch_bounds__(32 * (NWC + 1), zm_min_blocks<T, TY, NWC, LB>())
 zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                   const __grid_constant__ CUtensorMap tm_row,
                   const __grid_constant__ CUtensorMap tm_side, T* __restrict__ o,
                   const float* __restrict__ b, ZmGeom g, float c0, float c1, int* err) {
-    using C = ZmCfg<T, TY, NWC, STAGES>;
+    using C = ZmCfg<T, TY, NWC, STAGES, LB>;
     constexpr int V = C::V, TX = C::TX, HX = C::HX, RW = C::RW;
     static_assert(V % 2 == 0, "lanes hold whole float2 pairs");
     extern __shared__ __align__(128) unsigned char smem[];
@@ -161,13 +163,14 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
 
     if (warp == NWC) {
         if (lane == 0)
-            zm_produce<T, PER, TY, NWC, STAGES>(&tm_body, &tm_row, &tm_side, g, smem, full,
-                                                empty, issued, err);
+            zm_produce<T, PER, TY, NWC, STAGES, LB>(&tm_body, &tm_row, &tm_side, g, smem, full,
+                                                    empty, issued, err);
         return;
     }
 
     // --------------------------------------------------------------------- consumer warps
-    using PK = Pack16<T>;
+    using PK = PackLane<T, LB>;
+    using LW = typename PK::W;  // one lane's vector
     constexpr int NP = PK::NP;  // float2 pairs per lane (V / 2)
     const int r0 = warp * RW;   // first tile row of this warp
     const float2 c0v = make_float2(c0, c0), c1v = make_float2(c1, c1);
@@ -181,8 +184,8 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
         ++it;
     };
     bool ok = true;
-    auto stage_row = [&](int s, int row) -> const uint4* {
-        return reinterpret_cast<const uint4*>(smem + s * C::STAGE_BYTES + row * TX * int(sizeof(T))) +
+    auto stage_row = [&](int s, int row) -> const LW* {
+        return reinterpret_cast<const LW*>(smem + s * C::STAGE_BYTES + row * TX * int(sizeof(T))) +
                lane;
     };
     auto side = [&](int s, int right) -> const T* {
@@ -225,7 +228,7 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
         for (int r = 0; r < RW; ++r)
             boff[r] = min(y0 + r0 + r, g.ny - 1) * g.nx + min(gx, g.nx - V);
         SrcRows<RW, V> bnext;
-        if (b != nullptr) bnext.load(b, int64_t(zlo) * P, boff);
+        if constexpr (SRC) bnext.load(b, int64_t(zlo) * P, boff);
 
         // plane zlo-1: only the own values are needed
         {
@@ -252,7 +255,7 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
 #pragma unroll
             for (int r = 0; r < RW; ++r) PK::unpack(*stage_row(sa, r0 + r + 1), abv[r]);
             SrcRows<RW, V> bcur;
-            if (b != nullptr) {
+            if constexpr (SRC) {
                 bcur = bnext;
                 if (z + 1 < zhi) bnext.load(b, int64_t(z + 1) * P, boff);
             }
@@ -271,7 +274,7 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                 const float xlv = lane == 0 ? to_f(sl[(r0 + r) * HX + HX - 1]) : left;
                 const float xrv = (lane == 31 || wrapx) ? to_f(sr[(r0 + r) * HX]) : right;
                 float2 bv[NP];
-                if (b != nullptr) {
+                if constexpr (SRC) {
 #pragma unroll
                     for (int q = 0; q < NP / 2; ++q) {
                         const float4 t4 = bcur.v[r][q];
@@ -296,7 +299,7 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                     float2 v;
                     if constexpr (PACKED) {
                         v = upd3_sx2(c0v, c1v, ctr[r][p], sx[p], ym, yp, bel[r][p], abv[r][p]);
-                        if (b != nullptr) v = add2(v, bv[p]);
+                        if constexpr (SRC) v = add2(v, bv[p]);
                     } else {  // scalar chain, same rounding
                         const float sx0 = __fadd_rn(__fadd_rn(sx[p].x, __fadd_rn(ym.x, yp.x)),
                                                     __fadd_rn(bel[r][p].x, abv[r][p].x));
@@ -304,7 +307,7 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                                                     __fadd_rn(bel[r][p].y, abv[r][p].y));
                         v.x = __fadd_rn(__fmul_rn(c0, ctr[r][p].x), __fmul_rn(c1, sx0));
                         v.y = __fadd_rn(__fmul_rn(c0, ctr[r][p].y), __fmul_rn(c1, sx1));
-                        if (b != nullptr) {
+                        if constexpr (SRC) {
                             v.x = __fadd_rn(v.x, bv[p].x);
                             v.y = __fadd_rn(v.y, bv[p].y);
                         }
@@ -314,7 +317,7 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                 if (!((skipy >> r) & 1u)) {
                     T* dst = o + int64_t(z) * P + int64_t(gy) * g.nx + gx;
                     if (skipx == 0) {
-                        *reinterpret_cast<uint4*>(dst) = PK::pack(out);
+                        *reinterpret_cast<LW*>(dst) = PK::pack(out);
                     } else {
 #pragma unroll
                         for (int p = 0; p < NP; ++p) {
@@ -898,12 +901,14 @@ cudaError_t ring3d_cfg(const Launch& L, int variant) {
 }
 
 // FORM: 0 the register-capped packed/scalar consumer, 1 the first scalar consumer.
-template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED = true, int FORM = 0>
-cudaError_t zmarch_t(const Launch& L) {
-    using C = ZmCfg<T, TY, NWC, STAGES>;
+template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED = true, int FORM = 0,
+          int LB = 16, bool SRC = true>
+cudaError_t zmarch_t_src(const Launch& L) {
+    static_assert(FORM == 0 || LB == 16, "the first consumer form takes 16-byte lanes");
+    using C = ZmCfg<T, TY, NWC, STAGES, LB>;
     auto pick = [] {
         if constexpr (FORM == 1) return zmarch_v1_kernel<T, PER, TY, NWC, STAGES>;
-        else return zmarch_tma_kernel<T, PER, TY, NWC, STAGES, PACKED>;
+        else return zmarch_tma_kernel<T, PER, TY, NWC, STAGES, PACKED, LB, SRC>;
     };
     auto kern = pick();
     static std::atomic<int> blocks_per_sm[64];  // per device; first calls may race harmlessly
@@ -963,6 +968,16 @@ cudaError_t zmarch_t(const Launch& L) {
     return cudaGetLastError();
 }
 
+// The Jacobi source term is a compile-time choice for the register-capped consumer: without it
+// the consumers carry no source prefetch registers.
+template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED = true, int FORM = 0,
+          int LB = 16>
+cudaError_t zmarch_t(const Launch& L) {
+    if (FORM == 1 || L.src != nullptr)
+        return zmarch_t_src<T, PER, TY, NWC, STAGES, PACKED, FORM, LB, true>(L);
+    return zmarch_t_src<T, PER, TY, NWC, STAGES, PACKED, FORM, LB, false>(L);
+}
+
 }  // namespace
 
 bool zmarch_tma_supported(const Launch& L) {
@@ -972,11 +987,14 @@ bool zmarch_tma_supported(const Launch& L) {
            L.nx >= int(16 / es) && get_encode() != nullptr;
 }
 
-// Compiled z-march configurations: rows per tile (TY), consumer warps (NWC), ring stages.
+// Compiled z-march configurations: rows per tile (TY), consumer warps (NWC), ring stages; L8:
+// 8-byte lanes for 16-bit storage (4 values per lane: tiles half as wide, twice the rows per
+// warp for the same registers; fp32 grids run the default configuration instead).
 static const char* kZmNames[] = {"TY16_W8_S6", "TY8_W8_S8", "TY32_W8_S4", "TY16_W16_S6",
                                  "TY8_W4_S8", "TY16_W8_S6_scalar", "TY16_W16_S6_scalar",
-                                 "TY16_W8_S6_v1", "TY16_W16_S6_v1"};
-constexpr int kZmCount = 9;
+                                 "TY16_W8_S6_v1", "TY16_W16_S6_v1", "TY32_W8_S6_L8",
+                                 "TY16_W8_S6_L8", "TY32_W16_S6_L8"};
+constexpr int kZmCount = 12;
 
 int zmarch_configs(const char** names, int max) {
     for (int i = 0; i < kZmCount && names != nullptr && i < max; ++i) names[i] = kZmNames[i];
@@ -998,6 +1016,16 @@ static cudaError_t zmarch_cfg(const Launch& L) {
         case 5: return zmarch_t<T, PER, 16, 8, 6, false>(L);
         case 6: return zmarch_t<T, PER, 16, 16, 6, false>(L);
         case 7: return zmarch_t<T, PER, 16, 8, 6, true, 1>(L);
+        // 8-byte lanes for 16-bit storage only (an fp32 lane would hold a single pair)
+        case 9:
+            if constexpr (sizeof(T) == 2) return zmarch_t<T, PER, 32, 8, 6, true, 0, 8>(L);
+            else return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
+        case 10:
+            if constexpr (sizeof(T) == 2) return zmarch_t<T, PER, 16, 8, 6, true, 0, 8>(L);
+            else return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
+        case 11:
+            if constexpr (sizeof(T) == 2) return zmarch_t<T, PER, 32, 16, 6, true, 0, 8>(L);
+            else return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
         default: return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
     }
 }

@@ -11,9 +11,14 @@ are admitted while a slot and the HBM budget allow. Requests that arrive while o
 GPU therefore join the very next round, and their work overlaps on the device.
 
 * heat request: ``steps`` FTCS updates; done when they are all applied;
-* Jacobi request: sweeps with a source until the relative change of one sweep
-  ``||u_k+1 - u_k|| / ||u_k+1||`` is at most ``tol`` (checked after each round; the two ping-pong
-  buffers hold the last two iterates) or ``max_sweeps`` is reached.
+* Jacobi request for A u = f (A the 2d+1-point Laplacian over h^2, Dirichlet zero walls): sweeps
+  ``u' = S(u)/(2d) + b`` with ``b = -h^2 f / (2d)`` until the relative residual
+  ``||f - A u|| / ||f||`` is at most ``tol`` or ``max_sweeps`` is reached. One sweep's change is
+  the scaled residual of the iterate it started from, ``u_k+1 - u_k = -(h^2/(2d)) (f - A u_k)``,
+  so the relative residual of u_k is ``||u_k+1 - u_k|| / ||b||``: the two ping-pong buffers hold
+  both iterates after each round and the norms are taken on the device (one synchronisation per
+  round for all Jacobi requests). With 16-bit storage the iterates are the stored (rounded)
+  values, whose residual stalls near the storage resolution; such requests end at the cap.
 
 Each result equals the same request run alone with the same step / sweep count, bit for bit: a
 problem's arithmetic does not depend on what else is in the batch.
@@ -53,7 +58,7 @@ class Request:
     storage: str
     r: float = 0.0                 # heat: mesh Fourier number
     steps: int = 0                 # heat: updates
-    tol: float = 0.0               # jacobi: relative-change tolerance
+    tol: float = 0.0               # jacobi: relative-residual tolerance
     max_sweeps: int = 20000        # jacobi: cap
     seed: int = 0
 
@@ -130,13 +135,14 @@ def poisson_stream(rate: float, duration: float, seed: int = 0, n2d=(64, 2048), 
 # GPU executor
 # ------------------------------------------------------------------------------------------
 class _Slot:
-    __slots__ = ("req", "a", "b", "src", "in_b", "done", "last_change")
+    __slots__ = ("req", "a", "b", "src", "in_b", "done", "last_change", "src_norm")
 
     def __init__(self, req, a, b, src):
         self.req, self.a, self.b, self.src = req, a, b, src
         self.in_b = False      # current state in b
         self.done = 0          # steps / sweeps applied
-        self.last_change = math.inf
+        self.last_change = math.inf  # Jacobi: relative residual of the previous iterate
+        self.src_norm = None   # Jacobi: ||b||, a device scalar (set at allocation)
 
 
 class GpuExecutor:
@@ -172,7 +178,10 @@ class GpuExecutor:
     def alloc(self, req: Request) -> _Slot:
         u, src = self.init_fields(req)
         a = u.to(getattr(self.torch, req.storage)).contiguous()
-        return _Slot(req, a, a.clone(), src)
+        slot = _Slot(req, a, a.clone(), src)
+        if src is not None:
+            slot.src_norm = src.norm()
+        return slot
 
     def advance(self, slots: list[_Slot], counts: list[int]) -> None:
         """One round: every slot advances by its count, in one persistent launch."""
@@ -210,15 +219,8 @@ class GpuExecutor:
             s.done += c
 
     def converged(self, s: _Slot) -> bool:
-        """Jacobi: relative change of the last sweep within tolerance (or the sweep cap hit)."""
-        if s.done == 0:
-            return False
-        cur, prev = (s.b, s.a) if s.in_b else (s.a, s.b)
-        cf = cur.float()
-        nrm = float(cf.norm())
-        diff = float((cf - prev.float()).norm())
-        s.last_change = diff / nrm if nrm > 0 else 0.0
-        return s.last_change <= s.req.tol
+        """Jacobi: relative residual ||f - A u|| / ||f|| of the previous iterate within tol."""
+        return self.converged_many([s])[0]
 
     def converged_many(self, slots: list[_Slot]) -> list[bool]:
         """:meth:`converged` for several slots with a single device synchronisation."""
@@ -228,12 +230,11 @@ class GpuExecutor:
         pairs = []
         for s in slots:
             cur, prev = (s.b, s.a) if s.in_b else (s.a, s.b)
-            cf = cur.float()
-            pairs.append(torch.stack([cf.norm(), (cf - prev.float()).norm()]))
+            pairs.append(torch.stack([(cur.float() - prev.float()).norm(), s.src_norm]))
         vals = torch.stack(pairs).cpu().tolist()
         out = []
-        for s, (nrm, diff) in zip(slots, vals):
-            s.last_change = diff / nrm if nrm > 0 else 0.0
+        for s, (diff, bn) in zip(slots, vals):
+            s.last_change = diff / bn if bn > 0 else 0.0
             out.append(s.done > 0 and s.last_change <= s.req.tol)
         return out
 
@@ -283,15 +284,29 @@ class ServeStats:
     backlog: int
     updates: int
     extra: dict = field(default_factory=dict)
+    #: arrival times of the requests that had arrived but not finished when the run ended
+    open_arrivals: list[float] = field(default_factory=list)
+
+    def latencies_all(self) -> list[float]:
+        """Latency of every arrived request: completed ones by latency, unfinished ones by
+        their age when the run ended (right-censored: a lower bound of their latency)."""
+        return [o.latency for o in self.outcomes] + [max(0.0, self.wall - a)
+                                                      for a in self.open_arrivals]
 
     def summary(self) -> dict:
-        lat = np.array([o.latency for o in self.outcomes]) if self.outcomes else np.array([np.nan])
+        lat_done = (np.array([o.latency for o in self.outcomes]) if self.outcomes
+                    else np.array([np.nan]))
+        lat_all = np.array(self.latencies_all() or [np.nan])
         return {
             "completed": len(self.outcomes), "submitted": self.submitted,
             "backlog": self.backlog, "wall_s": round(self.wall, 3),
             "solves_per_s": round(len(self.outcomes) / self.wall, 2) if self.wall > 0 else 0.0,
-            "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
-            "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
+            # over every arrived request; unfinished ones count with their age at the end
+            "p50_ms": round(float(np.percentile(lat_all, 50)) * 1e3, 2),
+            "p99_ms": round(float(np.percentile(lat_all, 99)) * 1e3, 2),
+            "censored": len(self.open_arrivals),
+            "completed_p50_ms": round(float(np.percentile(lat_done, 50)) * 1e3, 2),
+            "completed_p99_ms": round(float(np.percentile(lat_done, 99)) * 1e3, 2),
             "glups": round(self.updates / self.wall / 1e9, 2) if self.wall > 0 else 0.0,
             "rounds": self.rounds, "peak_hbm_gb": round(self.peak_bytes / 1e9, 2),
             "jacobi_converged": sum(o.converged for o in self.outcomes if o.kind == "jacobi"),
@@ -311,12 +326,13 @@ class Server:
 
     def __init__(self, executor, budget_bytes: float = 150e9, max_active: int = 1024,
                  quantum: int = 64, keep_results: bool = False, clock=time.perf_counter,
-                 sleep=time.sleep):
+                 sleep=time.sleep, keep_ids=()):
         self.ex = executor
         self.budget = float(budget_bytes)
         self.max_active = max_active
         self.quantum = quantum
         self.keep = keep_results
+        self.keep_ids = set(keep_ids)  # requests whose results are copied back in any case
         self.clock = clock
         self.sleep = sleep
 
@@ -384,7 +400,7 @@ class Server:
                     conv = conv_of[id(slot)]
                     fin = conv or slot.done >= req.max_sweeps
                 if fin:
-                    res = self.ex.fetch(slot) if self.keep else None
+                    res = self.ex.fetch(slot) if self.keep or req.rid in self.keep_ids else None
                     tnow = self.clock() - t0
                     outcomes.append(Outcome(req.rid, req.kind, req.arrival, adm, tnow, slot.done,
                                             conv, res))
@@ -395,7 +411,10 @@ class Server:
             active = still
         wall = self.clock() - t0
         backlog = len(arrived) + len(active) + (len(pending) - i)
-        return ServeStats(outcomes, wall, rounds, len(requests), peak, backlog, updates)
+        open_arr = [a for a, _, _ in arrived] + [s.req.arrival for s, _ in active] + [
+            r.arrival for r in pending[i:] if r.arrival <= wall]
+        return ServeStats(outcomes, wall, rounds, len(requests), peak, backlog, updates,
+                          open_arrivals=open_arr)
 
 
 class PlainServer:
@@ -406,10 +425,11 @@ class PlainServer:
     """
 
     def __init__(self, executor, quantum: int = 64, keep_results: bool = False,
-                 clock=time.perf_counter, sleep=time.sleep):
+                 clock=time.perf_counter, sleep=time.sleep, keep_ids=()):
         self.ex = executor
         self.quantum = quantum
         self.keep = keep_results
+        self.keep_ids = set(keep_ids)
         self.clock = clock
         self.sleep = sleep
 
@@ -444,14 +464,15 @@ class PlainServer:
                         conv = True
                         break
             self.ex.synchronize()
-            res = self.ex.fetch(slot) if self.keep else None
+            res = self.ex.fetch(slot) if self.keep or req.rid in self.keep_ids else None
             updates += req.cells * slot.done
             outcomes.append(Outcome(req.rid, req.kind, req.arrival, adm, self.clock() - t0,
                                     slot.done, conv, res))
             self.ex.free(slot)
         wall = self.clock() - t0
+        open_arr = [r.arrival for r in pending[len(outcomes):] if r.arrival <= wall]
         return ServeStats(outcomes, wall, len(outcomes), len(requests), peak,
-                          len(pending) - len(outcomes), updates)
+                          len(pending) - len(outcomes), updates, open_arrivals=open_arr)
 
 
 # ------------------------------------------------------------------------------------------
@@ -463,7 +484,8 @@ def shard(requests: list[Request], rank: int, world: int) -> list[Request]:
 
 
 def merge(stats: list[dict], latencies: list[list[float]]) -> dict:
-    """Whole-job summary from per-replica summaries and raw latencies (seconds)."""
+    """Whole-job summary from per-replica summaries and raw latencies (seconds; unfinished
+    requests by their age at the end, as :meth:`ServeStats.latencies_all`)."""
     lat = np.array([x for part in latencies for x in part]) if any(latencies) else np.array([0.0])
     wall = max(s["wall_s"] for s in stats)
     done = sum(s["completed"] for s in stats)
@@ -484,6 +506,5 @@ def gather_summary(local: ServeStats, group=None) -> dict:
 
     world = dist.get_world_size(group)
     parts: list = [None] * world
-    dist.all_gather_object(parts, (local.summary(), [o.latency for o in local.outcomes]),
-                           group=group)
+    dist.all_gather_object(parts, (local.summary(), local.latencies_all()), group=group)
     return merge([p[0] for p in parts], [p[1] for p in parts])

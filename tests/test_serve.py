@@ -205,3 +205,45 @@ def test_gpu_engine_and_plain_agree_on_a_stream():
     for rid in a:
         assert a[rid].steps_done == b[rid].steps_done
         assert np.array_equal(a[rid].result, b[rid].result)
+
+
+def test_censored_latencies_count_the_backlog():
+    """Requests still open at the end of a run count with their age (a lower bound)."""
+    clock = FakeClock()
+    ex = FakeExecutor(clock)
+    reqs = poisson_stream(2000.0, 0.05, seed=11)
+    stats = Server(ex, quantum=64, clock=clock, sleep=clock.sleep, max_active=4).run(
+        reqs, duration=0.05, drain=False)
+    s = stats.summary()
+    assert s["backlog"] > 0 and s["censored"] == len(stats.open_arrivals) > 0
+    lat = stats.latencies_all()
+    assert len(lat) == len(stats.outcomes) + s["censored"]
+    assert all(x >= 0 for x in lat)
+
+
+@pytest.mark.gpu
+def test_gpu_served_results_match_the_oracle():
+    """Every served result equals the oracle run on the same initial field for the same number
+    of steps / sweeps, with the storage rounding of a single-step kernel (emulated_reference,
+    k = 1): fp32 bit for bit, 16-bit storage bit for bit with its per-step rounding."""
+    import torch
+
+    from oracle import emulated_reference
+    from pyheat3d_b200.serve import GpuExecutor
+
+    ex = GpuExecutor()
+    reqs = poisson_stream(400.0, 0.05, seed=12, n2d=(16, 96), n3d=(8, 24), steps=(5, 90),
+                          tol=(1e-6, 1e-4), max_sweeps=320,
+                          storages=("float32", "bfloat16", "float16"))
+    assert len(reqs) >= 10
+    stats = Server(ex, quantum=32, keep_results=True).run(reqs)
+    assert len(stats.outcomes) == len(reqs)
+    for o in stats.outcomes:
+        req = reqs[o.rid]
+        u, src = ex.init_fields(req)  # regenerated from the request's seed on the device
+        u0 = u.cpu().numpy()
+        b = src.cpu().numpy() if src is not None else None
+        c0, c1 = req.coefficients()
+        want = emulated_reference(u0, c0, c1, req.bc, o.steps_done, req.storage, 1, b)
+        assert np.array_equal(o.result, want), (req, o.steps_done)
+    torch.cuda.synchronize()
