@@ -134,7 +134,7 @@ __device__ __forceinline__ void zm_produce(const CUtensorMap* tm_body, const CUt
 }
 
 template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED, int LB = 16,
-          bool SRC = true>
+          bool SRC = true, bool ROT = false>
 __global__ void __launch_bounds__(32 * (NWC + 1), zm_min_blocks<T, TY, NWC, LB>())
 zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                   const __grid_constant__ CUtensorMap tm_row,
@@ -247,11 +247,15 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
 #pragma unroll
         for (int r = 0; r < RW; ++r) PK::unpack(*stage_row(sc, r0 + r + 1), ctr[r]);
 
-        for (int z = zlo; z < zhi; ++z) {
+        // One plane z with the below / centre / above planes in the given register sets; the
+        // above set is loaded here. ROT rotates the three sets by name (three planes per loop
+        // pass, no register copies); otherwise the sets are copied down after every plane.
+        auto plane = [&](int z, float2 (&bel)[RW][NP], float2 (&ctr)[RW][NP],
+                         float2 (&abv)[RW][NP]) {
             int sa;
             uint32_t pha;
             take(sa, pha);
-            if (!mbar_wait(&full[sa], pha, err)) { ok = false; break; }
+            if (!mbar_wait(&full[sa], pha, err)) { ok = false; return; }
 #pragma unroll
             for (int r = 0; r < RW; ++r) PK::unpack(*stage_row(sa, r0 + r + 1), abv[r]);
             SrcRows<RW, V> bcur;
@@ -328,14 +332,29 @@ zmarch_tma_kernel(const __grid_constant__ CUtensorMap tm_body,
                 }
             }
             release(sc);
-#pragma unroll
-            for (int r = 0; r < RW; ++r)
-#pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                    bel[r][p] = ctr[r][p];
-                    ctr[r][p] = abv[r][p];
-                }
             sc = sa;
+        };
+        if constexpr (ROT) {
+            for (int z = zlo; z < zhi; z += 3) {
+                plane(z, bel, ctr, abv);
+                if (!ok || z + 1 >= zhi) break;
+                plane(z + 1, ctr, abv, bel);
+                if (!ok || z + 2 >= zhi) break;
+                plane(z + 2, abv, bel, ctr);
+                if (!ok) break;
+            }
+        } else {
+            for (int z = zlo; z < zhi; ++z) {
+                plane(z, bel, ctr, abv);
+                if (!ok) break;
+#pragma unroll
+                for (int r = 0; r < RW; ++r)
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) {
+                        bel[r][p] = ctr[r][p];
+                        ctr[r][p] = abv[r][p];
+                    }
+            }
         }
         if (!ok) break;
         release(sc);  // plane zhi
@@ -900,15 +919,16 @@ cudaError_t ring3d_cfg(const Launch& L, int variant) {
     }
 }
 
-// FORM: 0 the register-capped packed/scalar consumer, 1 the first scalar consumer.
+// FORM: 0 the register-capped packed/scalar consumer, 1 the first scalar consumer, 2 form 0
+// with the plane register sets rotated by name.
 template <typename T, bool PER, int TY, int NWC, int STAGES, bool PACKED = true, int FORM = 0,
           int LB = 16, bool SRC = true>
 cudaError_t zmarch_t_src(const Launch& L) {
-    static_assert(FORM == 0 || LB == 16, "the first consumer form takes 16-byte lanes");
+    static_assert(FORM != 1 || LB == 16, "the first consumer form takes 16-byte lanes");
     using C = ZmCfg<T, TY, NWC, STAGES, LB>;
     auto pick = [] {
         if constexpr (FORM == 1) return zmarch_v1_kernel<T, PER, TY, NWC, STAGES>;
-        else return zmarch_tma_kernel<T, PER, TY, NWC, STAGES, PACKED, LB, SRC>;
+        else return zmarch_tma_kernel<T, PER, TY, NWC, STAGES, PACKED, LB, SRC, FORM == 2>;
     };
     auto kern = pick();
     static std::atomic<int> blocks_per_sm[64];  // per device; first calls may race harmlessly
@@ -993,8 +1013,10 @@ bool zmarch_tma_supported(const Launch& L) {
 static const char* kZmNames[] = {"TY16_W8_S6", "TY8_W8_S8", "TY32_W8_S4", "TY16_W16_S6",
                                  "TY8_W4_S8", "TY16_W8_S6_scalar", "TY16_W16_S6_scalar",
                                  "TY16_W8_S6_v1", "TY16_W16_S6_v1", "TY32_W8_S6_L8",
-                                 "TY16_W8_S6_L8", "TY32_W16_S6_L8"};
-constexpr int kZmCount = 12;
+                                 "TY16_W8_S6_L8", "TY32_W16_S6_L8", "TY16_W16_S6_rot",
+                                 "TY8_W8_S8_rot", "TY16_W8_S6_rot", "TY16_W8_S6_L8_rot",
+                                 "TY8_W8_S8_L8_rot"};
+constexpr int kZmCount = 17;
 
 int zmarch_configs(const char** names, int max) {
     for (int i = 0; i < kZmCount && names != nullptr && i < max; ++i) names[i] = kZmNames[i];
@@ -1006,7 +1028,8 @@ static cudaError_t zmarch_cfg(const Launch& L) {
     int cfg = L.cfg;
     // defaults measured on a B200 at 512^3 (1000-step solves, median of 3): fp32 the scalar
     // consumer with 16 rows x 16 warps (720 GLUPS vs 686 packed), 16-bit the packed 16 x 16
-    if (cfg < 0 || cfg >= kZmCount) cfg = sizeof(T) == 4 ? 8 : 3;
+    // with the plane register sets rotated by name (bf16 1238 vs 1185, fp16 1236 vs 1089)
+    if (cfg < 0 || cfg >= kZmCount) cfg = sizeof(T) == 4 ? 8 : 12;
     switch (cfg) {
         case 0: return zmarch_t<T, PER, 16, 8, 6>(L);
         case 1: return zmarch_t<T, PER, 8, 8, 8>(L);
@@ -1025,6 +1048,15 @@ static cudaError_t zmarch_cfg(const Launch& L) {
             else return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
         case 11:
             if constexpr (sizeof(T) == 2) return zmarch_t<T, PER, 32, 16, 6, true, 0, 8>(L);
+            else return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
+        case 12: return zmarch_t<T, PER, 16, 16, 6, true, 2>(L);
+        case 13: return zmarch_t<T, PER, 8, 8, 8, true, 2>(L);
+        case 14: return zmarch_t<T, PER, 16, 8, 6, true, 2>(L);
+        case 15:
+            if constexpr (sizeof(T) == 2) return zmarch_t<T, PER, 16, 8, 6, true, 2, 8>(L);
+            else return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
+        case 16:
+            if constexpr (sizeof(T) == 2) return zmarch_t<T, PER, 8, 8, 8, true, 2, 8>(L);
             else return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
         default: return zmarch_t<T, PER, 16, 16, 6, true, 1>(L);
     }

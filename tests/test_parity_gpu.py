@@ -275,6 +275,8 @@ def test_every_compiled_config(storage, bc):
     u3c = rng.random((6, 9, 258), dtype=np.float32)
     marches = [(2, u2, st2, "b200/ymarch" + suf), (3, u3, st, "b200/zmarch" + suf),
                (3, u3b, st, "b200/zmarch" + suf), (3, u3c, st, "b200/zmarch" + suf)]
+    b3 = rng.random(u0.shape, dtype=np.float32) * np.float32(1e-2)
+    b2 = rng.random(u2.shape, dtype=np.float32) * np.float32(1e-2)
     try:
         for fam, k, key in cases:
             for cfg in range(L.ph3_tune_count(K[fam], 3, k)):
@@ -283,6 +285,20 @@ def test_every_compiled_config(storage, bc):
                     steps = 2 * k + 1
                     _assert_same(_run(key, u0, st, steps), _ref(key, u0, st, steps),
                                  (key, cfg, chunk))
+                if fam == "tb":  # the Jacobi source through every tb configuration
+                    _assert_same(_run(key, u0, st, k + 1, b3), _ref(key, u0, st, k + 1, b3),
+                                 (key, cfg, "source"))
+        # 2D temporal blocking: every configuration, with and without a source, odd chunks
+        for k in (2, 3, 4, 8):
+            key = f"b200/tb{k}" + suf
+            for cfg in range(L.ph3_tune_count(K["tb"], 2, k)):
+                for chunk in (0, 7):
+                    _lib.check(L.ph3_tune_set(K["tb"], 2, S, k, cfg, chunk))
+                    _assert_same(_run(key, u2, st2, 2 * k + 1), _ref(key, u2, st2, 2 * k + 1),
+                                 (key, "2d", cfg, chunk))
+                _assert_same(_run(key, u2, st2, k + 1, b2), _ref(key, u2, st2, k + 1, b2),
+                             (key, "2d", cfg, "source"))
+            L.ph3_tune_set(K["tb"], 2, S, k, -1, 0)
         for dims, u, stc, key in marches:
             bsrc = rng.random(u.shape, dtype=np.float32) if dims == 3 else None
             for cfg in range(L.ph3_tune_count(K["march"], dims, 1)):
