@@ -620,8 +620,13 @@ def bench_serving(torch, seconds: float) -> dict:
     from pyheat3d_b200.serve import GpuExecutor, PlainServer, Server, poisson_stream
 
     reqs = poisson_stream(2000.0, seconds, seed=0)
-    cost = sorted(reqs, key=lambda r: r.cells * (r.steps if r.kind == "heat" else r.max_sweeps))
-    keep = {r.rid for r in cost[: max(40, len(reqs) // 50)]}
+    # the smallest requests of each kind and storage (their results are copied back)
+    keep: set[int] = set()
+    for kind in ("heat", "jacobi"):
+        for storage in ("float32", "bfloat16"):
+            group = sorted((r for r in reqs if r.kind == kind and r.storage == storage),
+                           key=lambda r: r.cells)
+            keep.update(r.rid for r in group[:60])
     ex = GpuExecutor()
     eng_stats = Server(ex, budget_bytes=150e9, max_active=256, quantum=128, keep_ids=keep).run(
         reqs, duration=seconds, drain=False)

@@ -92,16 +92,25 @@ __device__ __noinline__ void run_tile(const BatchDesc& d, int s, int t) {
     const T* src = static_cast<const T*>((s & 1) ? d.b : d.a);
     T* dst = static_cast<T*>((s & 1) ? d.a : d.b);
     const int w = threadIdx.x >> 5;
+    // problems without a Jacobi source take tiles compiled without it
     if (d.dims == 3) {
         const int tx = t % d.ntx, ty = (t / d.ntx) % d.nty, tz = t / (d.ntx * d.nty);
-        const int z0 = tz * C::ZCH;
-        lite3d_item<T, PER, C::R, true>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1, tx,
-                                        (ty * kW + w) * C::R, z0, min(z0 + C::ZCH, d.nz));
+        const int z0 = tz * C::ZCH, z1 = min(z0 + C::ZCH, d.nz), y0 = (ty * kW + w) * C::R;
+        if (d.src != nullptr)
+            lite3d_item<T, PER, C::R, true, true>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1,
+                                                  tx, y0, z0, z1);
+        else
+            lite3d_item<T, PER, C::R, true, false>(src, dst, nullptr, d.nz, d.ny, d.nx, d.c0,
+                                                   d.c1, tx, y0, z0, z1);
     } else {
         const int tx = t % d.ntx, ty = t / d.ntx;
-        const int y0 = ty * C::YCH;
-        lite2d_item<T, PER, C::RB2, true>(src, dst, d.src, d.ny, d.nx, d.c0, d.c1, tx * kW + w,
-                                          y0, min(y0 + C::YCH, d.ny));
+        const int y0 = ty * C::YCH, y1 = min(y0 + C::YCH, d.ny);
+        if (d.src != nullptr)
+            lite2d_item<T, PER, C::RB2, true, true>(src, dst, d.src, d.ny, d.nx, d.c0, d.c1,
+                                                    tx * kW + w, y0, y1);
+        else
+            lite2d_item<T, PER, C::RB2, true, false>(src, dst, nullptr, d.ny, d.nx, d.c0, d.c1,
+                                                     tx * kW + w, y0, y1);
     }
 }
 

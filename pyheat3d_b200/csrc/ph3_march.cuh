@@ -436,7 +436,7 @@ __device__ __forceinline__ void march3d_item(const T* __restrict__ u, T* __restr
 // x-neighbours by shuffles (lane 0 / 31 hold the strip's halo column in one register per row)
 // and, in 3D, loads the rows just above and below its own rows directly.
 // ------------------------------------------------------------------------------------------
-template <typename T, bool PER, int R, bool CG>
+template <typename T, bool PER, int R, bool CG, bool SRC = true>
 __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restrict__ o,
                                             const float* __restrict__ b, int nz, int ny, int nx,
                                             float c0, float c1, int strip, int row0, int zlo,
@@ -473,7 +473,7 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
         for (int r = 0; r < R; ++r) {
             p.v[r] = ldx1<CG>(pl + roff[r] + cx);
             p.h[r] = hl ? ldx1<CG>(pl + roff[r] + hcol) : 0.f;
-            p.s[r] = b != nullptr ? __ldg(b + zo + roff[r] + cx) : 0.f;
+            p.s[r] = (SRC && b != nullptr) ? __ldg(b + zo + roff[r] + cx) : 0.f;
         }
         p.up = ldx1<CG>(pl + uoff + cx);
         p.dn = ldx1<CG>(pl + doff + cx);
@@ -504,7 +504,7 @@ __device__ __forceinline__ void lite3d_item(const T* __restrict__ u, T* __restri
             const float ym = r > 0 ? ctr.v[r - 1] : ctr.up;
             const float yp = r < R - 1 ? ctr.v[r + 1] : ctr.dn;
             float v = upd3(c0, c1, c, xm, xp, ym, yp, bel[r], abv.v[r]);
-            if (b != nullptr) v = __fadd_rn(v, ctr.s[r]);
+            if ((SRC && b != nullptr)) v = __fadd_rn(v, ctr.s[r]);
             if (!xskip && !((yskip >> r) & 1u)) opl[roff[r] + x] = from_f<T>(v);
         }
 #pragma unroll
@@ -680,7 +680,7 @@ __device__ __forceinline__ void avec3d_item(const T* __restrict__ u, T* __restri
     }
 }
 
-template <typename T, bool PER, int RB, bool CG>
+template <typename T, bool PER, int RB, bool CG, bool SRC = true>
 __device__ __forceinline__ void lite2d_item(const T* __restrict__ u, T* __restrict__ o,
                                             const float* __restrict__ b, int ny, int nx,
                                             float c0, float c1, int strip, int ylo, int yhi) {
@@ -725,7 +725,7 @@ __device__ __forceinline__ void lite2d_item(const T* __restrict__ u, T* __restri
             if (lane == 0) xm = wh[q + 1];
             if (lane == 31) xp = wh[q + 1];
             float v = upd2(c0, c1, c, xm, xp, win[q], win[q + 2]);
-            if (b != nullptr) v = __fadd_rn(v, __ldg(b + int64_t(yy) * nx + cx));
+            if ((SRC && b != nullptr)) v = __fadd_rn(v, __ldg(b + int64_t(yy) * nx + cx));
             if (!xskip) o[int64_t(yy) * nx + x] = from_f<T>(v);
         }
         if (more) {

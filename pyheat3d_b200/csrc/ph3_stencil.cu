@@ -94,14 +94,14 @@ march3d_k1_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __res
                                          blockIdx.z, zch, vec_i != 0, edge);
 }
 
-template <typename T, bool PER, int R, int W>
+template <typename T, bool PER, int R, int W, bool SRC = true>
 __global__ void __launch_bounds__(32 * W)
 lite3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
               int ny, int nx, float c0, float c1, int zch, int zb, int ze) {
     const int w = threadIdx.x >> 5;
     const int z0 = zb + blockIdx.z * zch;
-    lite3d_item<T, PER, R, false>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x,
-                                  (blockIdx.y * W + w) * R, z0, min(z0 + zch, ze));
+    lite3d_item<T, PER, R, false, SRC>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x,
+                                       (blockIdx.y * W + w) * R, z0, min(z0 + zch, ze));
 }
 
 template <typename T, bool PER, int R, int W>
@@ -114,13 +114,14 @@ avec3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restric
                                   (blockIdx.y * W + w) * R, z0, min(z0 + zch, ze));
 }
 
-template <typename T, bool PER, int RB, int W>
+template <typename T, bool PER, int RB, int W, bool SRC = true>
 __global__ void __launch_bounds__(32 * W)
 lite2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int ny,
               int nx, float c0, float c1, int ych) {
     const int y0 = blockIdx.y * ych;
-    lite2d_item<T, PER, RB, false>(u, o, b, ny, nx, c0, c1, blockIdx.x * W + (threadIdx.x >> 5),
-                                   y0, min(y0 + ych, ny));
+    lite2d_item<T, PER, RB, false, SRC>(u, o, b, ny, nx, c0, c1,
+                                        blockIdx.x * W + (threadIdx.x >> 5), y0,
+                                        min(y0 + ych, ny));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -208,8 +209,12 @@ static cudaError_t march_k1_t(const Launch& L) {
                                         : default_chunk(L.ny, cdiv(strips, W), 8 * RB, 2 * target);
             dim3 grd(cdiv(strips, W), cdiv(L.ny, ych));
             if (grd.y > 65535) return cudaErrorInvalidConfiguration;
-            lite2d_kernel<T, PER, RB, W><<<grd, 32 * W, 0, L.stream>>>(u, o, L.src, L.ny, L.nx,
-                                                                      L.c0, L.c1, ych);
+            if (L.src != nullptr)
+                lite2d_kernel<T, PER, RB, W, true><<<grd, 32 * W, 0, L.stream>>>(
+                    u, o, L.src, L.ny, L.nx, L.c0, L.c1, ych);
+            else
+                lite2d_kernel<T, PER, RB, W, false><<<grd, 32 * W, 0, L.stream>>>(
+                    u, o, nullptr, L.ny, L.nx, L.c0, L.c1, ych);
         } else {
             constexpr int R = 4, W = 4;
             // planes zb .. ze-1 (a z range never wraps: its neighbour planes are in the array)
@@ -218,8 +223,12 @@ static cudaError_t march_k1_t(const Launch& L) {
             const int zch = L.chunk > 0 ? L.chunk : default_chunk(ze - zb, tiles, 16, 2 * target);
             dim3 grd(cdiv(L.nx, 32), cdiv(L.ny, W * R), cdiv(ze - zb, zch));
             if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
-            lite3d_kernel<T, PER, R, W><<<grd, 32 * W, 0, L.stream>>>(
-                u, o, L.src, L.nz, L.ny, L.nx, L.c0, L.c1, zch, zb, ze);
+            if (L.src != nullptr)
+                lite3d_kernel<T, PER, R, W, true><<<grd, 32 * W, 0, L.stream>>>(
+                    u, o, L.src, L.nz, L.ny, L.nx, L.c0, L.c1, zch, zb, ze);
+            else
+                lite3d_kernel<T, PER, R, W, false><<<grd, 32 * W, 0, L.stream>>>(
+                    u, o, nullptr, L.nz, L.ny, L.nx, L.c0, L.c1, zch, zb, ze);
         }
         return cudaGetLastError();
     }
