@@ -74,6 +74,12 @@ def parse() -> argparse.Namespace:
                          "local copies); on also runs it across ranks (NCCL halo exchange)")
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="length of the Poisson request stream (2000 req/s; 60 s configured)")
+    ap.add_argument("--batch-problems", type=int, default=512,
+                    help="problems of the batching measurement (512 configured; fewer only for "
+                         "profiling the batch kernel)")
+    ap.add_argument("--precision-n", type=int, default=256,
+                    help="grid edge of the precision measurement (256 configured; smaller only "
+                         "for profiling the defect-correction kernels)")
     ap.add_argument("--variant", default="b200/zmarch",
                     help="kernel of the headline line (b200/zmarch; others for profiling)")
     ap.add_argument("--n", type=int, default=None,
@@ -455,8 +461,10 @@ def run_b200(a: argparse.Namespace) -> None:
         extra["zslab"] = bench_zslab(torch, ws, rank, min(T, 200), value / ws)
         torch.cuda.empty_cache()
     if ws == 1:
-        for name, flag, fn in (("precision", a.no_precision, lambda: bench_precision(torch)),
-                               ("batching", a.no_batch, lambda: bench_batching(torch)),
+        for name, flag, fn in (("precision", a.no_precision,
+                                lambda: bench_precision(torch, a.precision_n)),
+                               ("batching", a.no_batch,
+                                lambda: bench_batching(torch, a.batch_problems)),
                                ("serving", a.no_serve,
                                 lambda: bench_serving(torch, a.serve_seconds))):
             if flag:
@@ -542,7 +550,7 @@ def bench_zslab(torch, ws: int, rank: int, tsteps: int, per_rank_glups: float) -
 # ---------------------------------------------------------------------------------------------
 # precision, batching and serving workloads (1-GPU runs; reported beside the headline)
 # ---------------------------------------------------------------------------------------------
-def bench_batching(torch) -> dict:
+def bench_batching(torch, nprob: int = 512) -> dict:
     """512 uneven grids: one persistent launch in a CUDA graph vs per-grid launches."""
     import ctypes
 
@@ -550,7 +558,7 @@ def bench_batching(torch) -> dict:
     from pyheat3d_b200 import _lib
     from pyheat3d_b200.batch import Batch, synthetic_batch
 
-    probs = synthetic_batch(512, seed=0)
+    probs = synthetic_batch(nprob, seed=0)
     batch = Batch(probs)
     upd = batch.updates
     g = batch.graph(with_reset=True)

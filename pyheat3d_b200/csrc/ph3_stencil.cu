@@ -17,31 +17,35 @@
 namespace ph3 {
 
 // ------------------------------------------------------------------------------------------
-// naive: one lattice site per thread; every operand through L1/L2
+// naive: one lattice site per thread; every operand through L1/L2. The site's offset is formed
+// once; the neighbours are signed deltas from it (+-1, +-nx, +-nx*ny), replaced by the wrapped
+// delta only on the periodic boundary, so a site costs seven loads, the update and one store.
 // ------------------------------------------------------------------------------------------
-template <typename T, bool PER>
+template <typename T, bool PER, bool SRC>
 __global__ void __launch_bounds__(256)
 naive2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int ny,
                int nx, float c0, float c1) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= nx || j >= ny) return;
-    int im, ip, jm, jp;
-    if constexpr (PER) {
-        im = i == 0 ? nx - 1 : i - 1; ip = i == nx - 1 ? 0 : i + 1;
-        jm = j == 0 ? ny - 1 : j - 1; jp = j == ny - 1 ? 0 : j + 1;
-    } else {
+    if constexpr (!PER) {
         if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1) return;
-        im = i - 1; ip = i + 1; jm = j - 1; jp = j + 1;
     }
-    const int64_t r = int64_t(j) * nx;
-    float v = upd2(c0, c1, ldg1(u + r + i), ldg1(u + r + im), ldg1(u + r + ip),
-                   ldg1(u + int64_t(jm) * nx + i), ldg1(u + int64_t(jp) * nx + i));
-    if (b != nullptr) v = __fadd_rn(v, __ldg(b + r + i));
-    o[r + i] = from_f<T>(v);
+    const int64_t c = int64_t(j) * nx + i;
+    int64_t xm = -1, xp = 1, ym = -int64_t(nx), yp = nx;
+    if constexpr (PER) {
+        if (i == 0) xm = nx - 1;
+        if (i == nx - 1) xp = 1 - nx;
+        if (j == 0) ym = int64_t(ny - 1) * nx;
+        if (j == ny - 1) yp = -int64_t(ny - 1) * nx;
+    }
+    const T* p = u + c;
+    float v = upd2(c0, c1, ldg1(p), ldg1(p + xm), ldg1(p + xp), ldg1(p + ym), ldg1(p + yp));
+    if constexpr (SRC) v = __fadd_rn(v, __ldg(b + c));
+    o[c] = from_f<T>(v);
 }
 
-template <typename T, bool PER>
+template <typename T, bool PER, bool SRC>
 __global__ void __launch_bounds__(256)
 naive3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
                int ny, int nx, float c0, float c1) {
@@ -49,24 +53,25 @@ naive3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restri
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i >= nx || j >= ny || k >= nz) return;
-    int im, ip, jm, jp, km, kp;
-    if constexpr (PER) {
-        im = i == 0 ? nx - 1 : i - 1; ip = i == nx - 1 ? 0 : i + 1;
-        jm = j == 0 ? ny - 1 : j - 1; jp = j == ny - 1 ? 0 : j + 1;
-        km = k == 0 ? nz - 1 : k - 1; kp = k == nz - 1 ? 0 : k + 1;
-    } else {
+    if constexpr (!PER) {
         if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1 || k == 0 || k == nz - 1) return;
-        im = i - 1; ip = i + 1; jm = j - 1; jp = j + 1; km = k - 1; kp = k + 1;
     }
     const int64_t P = int64_t(nx) * ny;
-    const int64_t c = int64_t(k) * P + int64_t(j) * nx;
-    float v = upd3(c0, c1, ldg1(u + c + i), ldg1(u + c + im), ldg1(u + c + ip),
-                   ldg1(u + int64_t(k) * P + int64_t(jm) * nx + i),
-                   ldg1(u + int64_t(k) * P + int64_t(jp) * nx + i),
-                   ldg1(u + int64_t(km) * P + int64_t(j) * nx + i),
-                   ldg1(u + int64_t(kp) * P + int64_t(j) * nx + i));
-    if (b != nullptr) v = __fadd_rn(v, __ldg(b + c + i));
-    o[c + i] = from_f<T>(v);
+    const int64_t c = int64_t(k) * P + int64_t(j) * nx + i;
+    int64_t xm = -1, xp = 1, ym = -int64_t(nx), yp = nx, zm = -P, zp = P;
+    if constexpr (PER) {
+        if (i == 0) xm = nx - 1;
+        if (i == nx - 1) xp = 1 - nx;
+        if (j == 0) ym = P - nx;
+        if (j == ny - 1) yp = nx - P;
+        if (k == 0) zm = (nz - 1) * P;
+        if (k == nz - 1) zp = -(nz - 1) * P;
+    }
+    const T* p = u + c;
+    float v = upd3(c0, c1, ldg1(p), ldg1(p + xm), ldg1(p + xp), ldg1(p + ym), ldg1(p + yp),
+                   ldg1(p + zm), ldg1(p + zp));
+    if constexpr (SRC) v = __fadd_rn(v, __ldg(b + c));
+    o[c] = from_f<T>(v);
 }
 
 template <typename T, bool PER, int V, int W, int RB>
@@ -148,12 +153,21 @@ static cudaError_t naive_t(const Launch& L) {
     if (L.dims == 2) {
         dim3 blk(32, 8), grd(cdiv(L.nx, 32), cdiv(L.ny, 8));
         if (grd.y > 65535) return cudaErrorInvalidConfiguration;
-        naive2d_kernel<T, PER><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.ny, L.nx, L.c0, L.c1);
+        if (L.src != nullptr)
+            naive2d_kernel<T, PER, true><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.ny, L.nx, L.c0,
+                                                                    L.c1);
+        else
+            naive2d_kernel<T, PER, false><<<grd, blk, 0, L.stream>>>(u, o, nullptr, L.ny, L.nx,
+                                                                     L.c0, L.c1);
     } else {
         dim3 blk(32, 4, 2), grd(cdiv(L.nx, 32), cdiv(L.ny, 4), cdiv(L.nz, 2));
         if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
-        naive3d_kernel<T, PER><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.nz, L.ny, L.nx, L.c0,
-                                                          L.c1);
+        if (L.src != nullptr)
+            naive3d_kernel<T, PER, true><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.nz, L.ny, L.nx,
+                                                                    L.c0, L.c1);
+        else
+            naive3d_kernel<T, PER, false><<<grd, blk, 0, L.stream>>>(u, o, nullptr, L.nz, L.ny,
+                                                                     L.nx, L.c0, L.c1);
     }
     return cudaGetLastError();
 }

@@ -120,6 +120,8 @@ class DefectCorrection:
         else:
             self.nz, self.ny, self.nx = self.shape
         self.c1 = float(np.float32(1.0 / (2 * self.dims)))
+        self.use_graph = True
+        self._graphs: dict[int, tuple] = {}
 
     def _stream(self):
         return _torch().cuda.current_stream(self.device).cuda_stream
@@ -132,8 +134,11 @@ class DefectCorrection:
         return max(float(self.rn2.item()), 0.0)
 
     def residual(self) -> float:
-        """Relative residual ||f - A u|| / ||f|| of the current u."""
-        self._rn2 = self._residual(1.0, False)
+        """Relative residual ||f - A u|| / ||f|| of the current u. The same pass also leaves
+        the unscaled correction source b = -h^2 r / (2d) in ``self.b`` for the next inner solve
+        (``self._b_scale`` = 1), so an outer iteration needs one FP64 residual pass."""
+        self._rn2 = self._residual(1.0, True)
+        self._b_scale = 1.0
         return math.sqrt(self._rn2) / self.fnorm
 
     def inner(self, m: int, rn2: float | None = None) -> None:
@@ -144,23 +149,53 @@ class DefectCorrection:
         ``rn2``: sum(r^2) of the current u if already known (saves one residual pass).
         """
         ncore = int(np.prod([x - 2 for x in self.shape]))
-        if rn2 is None:
-            rn2 = self._residual(1.0, False)
+        if rn2 is None or getattr(self, "_b_scale", None) != 1.0:
+            rn2 = self._residual(1.0, True)
         rms = math.sqrt(rn2 / ncore)
         sc = math.ldexp(1.0, math.floor(math.log2(rms))) if rms > 0 and math.isfinite(rms) \
             else 1.0
-        self._residual(1.0 / sc, True)
+        # b of the scaled equation: the unscaled source times 1/sc, a power of two, so the
+        # product is exact wherever b stays a normal fp32 number
+        self.b.mul_(1.0 / sc)
+        self._b_scale = 1.0 / sc
+        # the inner solve starts from e = 0; the other buffer's boundary layer is zero from the
+        # start and never written, its interior is overwritten by the first sweep
         self.ea.zero_()
-        self.eb.zero_()
+        e = self._sweeps(int(m))
+        _lib.check(self.lib.ph3_dc_correct(self.u.data_ptr(), e.data_ptr(),
+                                           _lib.STORAGE[self.storage], sc, e.numel(),
+                                           self._stream()))
+
+    def _advance(self, m: int) -> bool:
         in_b = ctypes.c_int(0)
         _lib.check(self.lib.ph3_advance(
             self.dims, self.nz, self.ny, self.nx, _lib.STORAGE[self.storage], _lib.BC["dirichlet"],
             0.0, self.c1, _lib.VARIANT[self.variant], self.k, self.ea.data_ptr(),
             self.eb.data_ptr(), self.b.data_ptr(), int(m), self._stream(), ctypes.byref(in_b)))
-        e = self.eb if in_b.value else self.ea
-        _lib.check(self.lib.ph3_dc_correct(self.u.data_ptr(), e.data_ptr(),
-                                           _lib.STORAGE[self.storage], sc, e.numel(),
-                                           self._stream()))
+        return bool(in_b.value)
+
+    def _sweeps(self, m: int):
+        """m inner sweeps from ea (buffers and source fixed for the whole solve); returns the
+        buffer holding the result. With ``use_graph`` the launch sequence of m sweeps is
+        captured once in a CUDA graph and replayed by later outer iterations: the inner
+        kernels are short (about 15 us at 256^3), so host-side launch work would otherwise
+        leave the GPU waiting between them."""
+        if not self.use_graph:
+            return self.eb if self._advance(m) else self.ea
+        torch = _torch()
+        g = self._graphs.get(m)
+        if g is None:
+            in_b = self._advance(m)  # warm-up outside capture (one-time kernel attributes)
+            self.ea.zero_()
+            side = torch.cuda.Stream(self.device)
+            side.wait_stream(torch.cuda.current_stream(self.device))
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=side):
+                in_b = self._advance(m)
+            torch.cuda.current_stream(self.device).wait_stream(side)
+            g = self._graphs[m] = (graph, in_b)
+        g[0].replay()
+        return self.eb if g[1] else self.ea
 
     def solve(self, tol: float = 1e-10, max_outer: int | None = None,
               sweeps: int | list[int] | None = None, max_sweeps: int | None = None) -> DCResult:

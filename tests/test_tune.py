@@ -100,5 +100,7 @@ def test_committed_table_picks_tb4_for_1024_cubed_fp32():
     """The committed table's b200/auto choice depends on the grid size (measured on a B200)."""
     t = tune.Table.load(tune.DEFAULT_TABLE)
     assert t.best_for(3, "float32", 1024 ** 3)["k"] == 4
-    assert t.best_for(3, "float32", 512 ** 3)["k"] == 1
+    assert t.best_for(3, "float32", 512 ** 3)["k"] == 4
+    assert t.best_for(3, "float32", 256 ** 3)["k"] == 1  # tiles too few to fill the GPU
+    assert t.best_for(3, "bfloat16", 512 ** 3)["k"] == 1
     assert t.best_for(2, "float32", 16384 ** 2)["k"] == 8
