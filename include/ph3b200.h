@@ -169,8 +169,11 @@ int ph3_dc_correct(double* u, const void* e, int storage, double e_scale, int64_
  * cupy_backend.py:183-194). Results equal the single-grid entry points bit for bit.
  *
  * Each ph3_problem names a ping-pong pair (a holds the initial state; with PH3_DIRICHLET, b must
- * hold the same boundary values), the grid, the coefficients and the number of steps. After the
- * launch a problem's state is in `a` when `steps` is even, else in `b`.
+ * hold the same boundary values), the grid, the coefficients, the number of steps and `k`: 0 or 1
+ * advance the problem by single steps; 2 or 4 (2D problems only) by steps / k passes of k
+ * fused steps each and then steps % k single steps (temporal blocking: 16-bit storage rounds
+ * once per pass, as ph3_advance with a tb variant). After the launch a problem's state is in `a`
+ * when its number of passes (steps, or steps / k + steps % k) is even, else in `b`.
  *
  * ph3_batch_workspace_bytes: device workspace (plan + counters) the problem list needs.
  * ph3_batch_prepare: validate the problems, build the plan and upload it into `ws` (synchronises
@@ -186,7 +189,7 @@ typedef struct ph3_problem {
     int32_t bc, storage;
     float c0, c1;
     int32_t steps;
-    int32_t reserved; /* must be 0 */
+    int32_t k; /* fused steps per pass: 0 or 1, or 2 / 4 for 2D problems */
 } ph3_problem;
 
 int64_t ph3_batch_workspace_bytes(const ph3_problem* problems, int n);

@@ -38,7 +38,7 @@ class ProblemDesc(ctypes.Structure):
                 ("dims", ctypes.c_int32), ("nz", ctypes.c_int32), ("ny", ctypes.c_int32),
                 ("nx", ctypes.c_int32), ("bc", ctypes.c_int32), ("storage", ctypes.c_int32),
                 ("c0", ctypes.c_float), ("c1", ctypes.c_float), ("steps", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("k", ctypes.c_int32)]
 
 
 @dataclass
@@ -50,6 +50,12 @@ class Problem:
     steps: int
     storage: str = "float32"
     source: np.ndarray | None = None
+    k: int = 1  # fused steps per pass: 1, or 2 / 4 for 2D grids
+
+    @property
+    def passes(self) -> int:
+        """Passes over the grid: steps, or steps // k fused passes and steps % k single steps."""
+        return self.steps // self.k + self.steps % self.k if self.k > 1 else self.steps
 
     @property
     def cells(self) -> int:
@@ -95,7 +101,7 @@ class Batch:
             d.c0 = float(np.float32(p.stencil.c0))
             d.c1 = float(np.float32(p.stencil.c1))
             d.steps = int(p.steps)
-            d.reserved = 0
+            d.k = int(p.k)
         self.n = n
         from .tune import configure_batch
 
@@ -145,7 +151,7 @@ class Batch:
 
     def result_tensor(self, i: int):
         """Device tensor holding problem i's final state."""
-        return self.b[i] if self.problems[i].steps % 2 else self.a[i]
+        return self.b[i] if self.problems[i].passes % 2 else self.a[i]
 
     def results(self) -> list[np.ndarray]:
         return [self.result_tensor(i).float().cpu().numpy() for i in range(self.n)]

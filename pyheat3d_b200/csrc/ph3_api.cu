@@ -410,7 +410,10 @@ int ph3_batch_prepare(const ph3_problem* problems, int n, void* ws, int64_t ws_b
             return fail(rc, "problem %d: %s", i, msg);
         }
         if (p.steps < 0) return fail(PH3_EINVAL, "problem %d: steps must be >= 0", i);
-        if (p.reserved != 0) return fail(PH3_EINVAL, "problem %d: reserved must be 0", i);
+        if (p.k != 0 && p.k != 1 && p.k != 2 && p.k != 4)
+            return fail(PH3_EINVAL, "problem %d: k must be 0, 1, 2 or 4, got %d", i, p.k);
+        if (p.k > 1 && p.dims != 2)
+            return fail(PH3_EINVAL, "problem %d: k = %d needs a 2D problem", i, p.k);
     }
     const long long need = batch_workspace_bytes(problems, n);
     if (ws_bytes < need)
@@ -424,7 +427,9 @@ int ph3_batch_prepare(const ph3_problem* problems, int n, void* ws, int64_t ws_b
 
 int ph3_batch_launch(void* ws, int n, void* stream) {
     if (ws == nullptr || n < 0) return fail(PH3_EINVAL, "ws must be non-null and n >= 0");
-    return finish(batch_launch(ws, n, status_ptr(), static_cast<cudaStream_t>(stream)),
+    tune_init();
+    const int cfg = g_tune_cfg[kFamBatch][1][PH3_FLOAT32][1].load();
+    return finish(batch_launch(ws, n, status_ptr(), static_cast<cudaStream_t>(stream), cfg),
                   "batch launch");
 }
 
@@ -441,7 +446,10 @@ int ph3_batch_run_static(const ph3_problem* problems, int n, void* stream) {
             return fail(rc, "problem %d: %s", i, msg);
         }
         if (p.steps < 0) return fail(PH3_EINVAL, "problem %d: steps must be >= 0", i);
-        if (p.reserved != 0) return fail(PH3_EINVAL, "problem %d: reserved must be 0", i);
+        if (p.k != 0 && p.k != 1 && p.k != 2 && p.k != 4)
+            return fail(PH3_EINVAL, "problem %d: k must be 0, 1, 2 or 4, got %d", i, p.k);
+        if (p.k > 1 && p.dims != 2)
+            return fail(PH3_EINVAL, "problem %d: k = %d needs a 2D problem", i, p.k);
     }
     long long need = 0;
     tune_init();

@@ -11,8 +11,12 @@
 // for later items, so the launch always makes progress.
 //
 // Tiles are the lean one-column-per-lane marches of ph3_march.cuh (any row alignment, no block
-// barrier inside a tile). Field reads go through L2 only (__ldcg): other blocks of the same
-// launch write the fields.
+// barrier inside a tile). A 2D problem with k > 1 advances by passes of k fused steps instead:
+// its items are (problem, pass, tile) and its tiles are eight warps of the 2D temporal-blocking
+// wavefront (ph3_tb2d.cuh, element loads), one overlapped column strip and a chunk of rows per
+// warp, followed by steps % k single-step passes over the same strips; the round numbering then
+// counts passes. Field reads go through L2 only (__ldcg): other
+// blocks of the same launch write the fields.
 // The item list is implicit: a plan in device memory (problem descriptors, the problems sorted
 // by steps, prefix sums of their tile counts and per-round item offsets) lets a block decode an
 // item number with two binary searches.
@@ -33,6 +37,7 @@
 #include "ph3_common.cuh"
 #include "ph3_internal.h"
 #include "ph3_march.cuh"
+#include "ph3_tb2d.cuh"
 
 namespace ph3 {
 
@@ -45,13 +50,15 @@ struct BatchDesc {
     int dims, nz, ny, nx, periodic, storage;
     float c0, c1;
     int steps;
-    int vec;
+    int k;       // fused steps per pass (1: single steps)
+    int fused;   // leading passes of k fused steps: steps / k
+    int passes;  // rounds this problem takes part in: steps / k, then steps % k single steps
     int ntx, nty, ntz, ntiles;
 };
 
 struct BatchHeader {
     int n;
-    int max_steps;
+    int max_steps;  // most passes of any problem (the number of rounds)
     int cfg;  // tile configuration the descriptors' tile counts were computed for
     int pad;
     long long total_items;
@@ -59,6 +66,23 @@ struct BatchHeader {
 };
 
 constexpr int kW = 8;  // warps per block
+constexpr int kTbRows = 256;  // rows per chunk of a 2D temporal-blocking tile
+
+// Lane widths of the batch's 2D temporal-blocking tiles (the batch kernel's register budget):
+// k = 2 takes 4 values per lane, k = 4 takes 2. The x halo is whole 16-byte granules, one granule
+// for every k up to 4 (and for the single-step remainder passes, which therefore cut a problem
+// into the same strips as its fused passes).
+template <int K> struct TbLane { static constexpr int V = K == 2 ? 4 : 2; };
+template <typename T, int K>
+__host__ __device__ constexpr int tb_strip_width() {  // stored columns per strip
+    return 32 * TbLane<K>::V - 2 * (((K + 16 / int(sizeof(T)) - 1) / (16 / int(sizeof(T)))) *
+                                    (16 / int(sizeof(T))));
+}
+static_assert(T2Cfg<float, 1, 4, 2>::OX == tb_strip_width<float, 2>() &&
+                  T2Cfg<float, 1, 2, 2>::OX == tb_strip_width<float, 4>() &&
+                  T2Cfg<__half, 1, 4, 2>::OX == tb_strip_width<__half, 2>() &&
+                  T2Cfg<__half, 1, 2, 2>::OX == tb_strip_width<__half, 4>(),
+              "remainder passes must cut the same strips as the fused passes");
 
 // Compiled tile configurations (the tuning table's batch family): rows per warp and planes per
 // 3D tile, rows per iteration and rows per 2D tile. The plan records which one it was built for.
@@ -66,8 +90,12 @@ template <int CFG> struct BCfg;
 template <> struct BCfg<0> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128; };
 template <> struct BCfg<1> { static constexpr int R = 2, ZCH = 16, RB2 = 4, YCH = 64; };
 template <> struct BCfg<2> { static constexpr int R = 8, ZCH = 64, RB2 = 8, YCH = 256; };
-constexpr int kBatchCfgs = 3;
-const char* kBatchNames[kBatchCfgs] = {"R4_Z32_Y128", "R2_Z16_Y64", "R8_Z64_Y256"};
+// Configurations 3 .. 5 are 0 .. 2 with the kernel compiled for two blocks per SM instead of
+// three (128 registers per thread instead of 80: the tile bodies no longer spill).
+constexpr int kBatchTiles = 3;
+constexpr int kBatchCfgs = 6;
+const char* kBatchNames[kBatchCfgs] = {"R4_Z32_Y128",    "R2_Z16_Y64",    "R8_Z64_Y256",
+                                       "R4_Z32_Y128_B2", "R2_Z16_Y64_B2", "R8_Z64_Y256_B2"};
 
 struct Geo { int R, ZCH, YCH; };
 Geo geo_of(int cfg) {
@@ -114,15 +142,52 @@ __device__ __noinline__ void run_tile(const BatchDesc& d, int s, int t) {
     }
 }
 
+// One item of a 2D problem with temporal blocking: eight strips (one per warp) of one chunk of
+// rows, pass s from buffer s % 2 into the other. KP fused steps in this pass (k, or 1 for the
+// remainder passes), lanes V wide as the problem's k sets.
+template <typename T, bool PER, int KP, int V, int KPROB>
+__device__ __noinline__ void run_tb2d_tile(const BatchDesc& d, int s, int t) {
+    const T* src = static_cast<const T*>((s & 1) ? d.b : d.a);
+    T* dst = static_cast<T*>((s & 1) ? d.a : d.b);
+    const int w = threadIdx.x >> 5;
+    const int tx = t % d.ntx, ty = t / d.ntx;
+    const int strip = tx * kW + w;
+    constexpr int OX = tb_strip_width<T, KPROB>();
+    const int nstrips = (d.nx + OX - 1) / OX;
+    if (strip >= nstrips) return;  // warp-uniform
+    const int y0 = ty * kTbRows, y1 = min(y0 + kTbRows, d.ny);
+    if (d.src != nullptr)
+        tb2d_pair_item<T, PER, true, false, KP, V, 2, true>(src, dst, d.src, d.ny, d.nx, strip, y0,
+                                                           y1, d.c0, d.c1, nullptr, nullptr,
+                                                           nullptr);
+    else
+        tb2d_pair_item<T, PER, false, false, KP, V, 2, true>(src, dst, nullptr, d.ny, d.nx, strip,
+                                                            y0, y1, d.c0, d.c1, nullptr, nullptr,
+                                                            nullptr);
+}
+
+template <typename T, bool PER, int CFG>
+__device__ __forceinline__ void run_problem_tile(const BatchDesc& d, int s, int t) {
+    if (d.k == 2) {
+        if (s < d.fused) run_tb2d_tile<T, PER, 2, TbLane<2>::V, 2>(d, s, t);
+        else run_tb2d_tile<T, PER, 1, TbLane<2>::V, 2>(d, s, t);
+    } else if (d.k == 4) {
+        if (s < d.fused) run_tb2d_tile<T, PER, 4, TbLane<4>::V, 4>(d, s, t);
+        else run_tb2d_tile<T, PER, 1, TbLane<4>::V, 4>(d, s, t);
+    } else {
+        run_tile<T, PER, CFG>(d, s, t);
+    }
+}
+
 template <int CFG>
 __device__ __forceinline__ void run_any(const BatchDesc& d, int s, int t) {
     switch (d.storage * 2 + d.periodic) {
-        case 0: run_tile<float, false, CFG>(d, s, t); break;
-        case 1: run_tile<float, true, CFG>(d, s, t); break;
-        case 2: run_tile<__half, false, CFG>(d, s, t); break;
-        case 3: run_tile<__half, true, CFG>(d, s, t); break;
-        case 4: run_tile<__nv_bfloat16, false, CFG>(d, s, t); break;
-        default: run_tile<__nv_bfloat16, true, CFG>(d, s, t); break;
+        case 0: run_problem_tile<float, false, CFG>(d, s, t); break;
+        case 1: run_problem_tile<float, true, CFG>(d, s, t); break;
+        case 2: run_problem_tile<__half, false, CFG>(d, s, t); break;
+        case 3: run_problem_tile<__half, true, CFG>(d, s, t); break;
+        case 4: run_problem_tile<__nv_bfloat16, false, CFG>(d, s, t); break;
+        default: run_problem_tile<__nv_bfloat16, true, CFG>(d, s, t); break;
     }
 }
 
@@ -136,7 +201,8 @@ __device__ __forceinline__ long long upper_bound_i64(const long long* a, int n, 
     return lo;
 }
 
-__global__ void __launch_bounds__(kThreads, 3)
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
     __shared__ int s_p, s_s, s_t;
     __shared__ long long s_item;
@@ -151,7 +217,7 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
     const long long* round_off = reinterpret_cast<const long long*>(base + hd->off_round);
     const long long total = hd->total_items;
     const int max_steps = hd->max_steps;
-    const int cfg = hd->cfg;
+    const int cfg = hd->cfg % kBatchTiles;
 
     for (;;) {
         if (threadIdx.x == 0) {
@@ -193,6 +259,7 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
     }
 }
 
+template <int MINB>
 int blocks_per_sm_cached() {
     // per device; concurrent first calls may both query, and store the same value atomically
     static std::atomic<int> nb[64];
@@ -200,7 +267,7 @@ int blocks_per_sm_cached() {
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
     int v = nb[dev].load(std::memory_order_acquire);
     if (v == 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, batch_kernel, kThreads, 0) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, batch_kernel<MINB>, kThreads, 0) !=
                 cudaSuccess ||
             v < 1)
             v = 1;
@@ -213,7 +280,21 @@ int cdiv(long long a, long long b) { return int((a + b - 1) / b); }
 
 // Geometry of one problem's tiles (must match run_tile / the item functions).
 void tiles_of(BatchDesc& d, int cfg) {
-    const Geo g = geo_of(cfg);
+    const Geo g = geo_of(cfg % kBatchTiles);
+    d.k = d.k > 1 ? d.k : 1;
+    d.fused = d.steps / d.k;
+    d.passes = d.fused + d.steps % d.k;
+    if (d.k > 1) {  // 2D temporal blocking: eight strips x one row chunk per item
+        int ox = 0;
+        const bool wide = d.storage == kF32;
+        if (d.k == 2) ox = wide ? tb_strip_width<float, 2>() : tb_strip_width<__half, 2>();
+        else ox = wide ? tb_strip_width<float, 4>() : tb_strip_width<__half, 4>();
+        d.ntx = cdiv(cdiv(d.nx, ox), kW);
+        d.nty = cdiv(d.ny, kTbRows);
+        d.ntz = 1;
+        d.ntiles = d.ntx * d.nty;
+        return;
+    }
     if (d.dims == 3) {
         d.ntx = cdiv(d.nx, 32);
         d.nty = cdiv(d.ny, kW * g.R);
@@ -224,7 +305,6 @@ void tiles_of(BatchDesc& d, int cfg) {
         d.ntz = 1;
     }
     d.ntiles = d.ntx * d.nty * d.ntz;
-    d.vec = 0;  // the lean tiles take any row alignment
 }
 
 struct Layout {
@@ -246,11 +326,16 @@ Layout layout_of(int n, int max_steps) {
 }  // namespace
 
 // -------------------------------------------------------------------------------- host API
-cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream);
+cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream, int cfg);
+
+// Passes of a problem: its steps, or steps / k fused passes and steps % k single steps.
+int passes_of(const ph3_problem& p) {
+    return p.k > 1 ? p.steps / p.k + p.steps % p.k : p.steps;
+}
 
 long long batch_workspace_bytes(const ph3_problem* p, int n) {
     int max_steps = 0;
-    for (int i = 0; i < n; ++i) max_steps = std::max(max_steps, p[i].steps);
+    for (int i = 0; i < n; ++i) max_steps = std::max(max_steps, passes_of(p[i]));
     return layout_of(n, max_steps).total;
 }
 
@@ -267,21 +352,22 @@ cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_by
         x.storage = p[i].storage;
         x.c0 = p[i].c0; x.c1 = p[i].c1;
         x.steps = p[i].steps;
+        x.k = p[i].k;
         tiles_of(x, cfg);
-        max_steps = std::max(max_steps, x.steps);
+        max_steps = std::max(max_steps, x.passes);
     }
     const Layout L = layout_of(n, max_steps);
     if (ws_bytes < L.total) return cudaErrorInvalidValue;
     std::vector<int> order(n);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return d[a].steps > d[b].steps; });
+                     [&](int a, int b) { return d[a].passes > d[b].passes; });
     std::vector<long long> tilepre(n + 1, 0);
     for (int q = 0; q < n; ++q) tilepre[q + 1] = tilepre[q] + d[order[q]].ntiles;
     std::vector<long long> round(max_steps + 1, 0);
     int active = n;
     for (int s = 0; s < max_steps; ++s) {
-        while (active > 0 && d[order[active - 1]].steps <= s) --active;
+        while (active > 0 && d[order[active - 1]].passes <= s) --active;
         round[s + 1] = round[s] + tilepre[active];
     }
     BatchHeader h;
@@ -362,7 +448,7 @@ cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t
                              long long* need_bytes, int cfg) {
     if (cfg < 0 || cfg >= kBatchCfgs) cfg = 0;
     int max_steps = 0;
-    for (int i = 0; i < n; ++i) max_steps = std::max(max_steps, p[i].steps);
+    for (int i = 0; i < n; ++i) max_steps = std::max(max_steps, passes_of(p[i]));
     const Layout L = layout_of(n, max_steps);
     if (need_bytes != nullptr) *need_bytes = L.total;
     if (L.total > kStaticWsBytes) return cudaErrorInvalidValue;
@@ -381,12 +467,13 @@ cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t
         x.storage = p[i].storage;
         x.c0 = p[i].c0; x.c1 = p[i].c1;
         x.steps = p[i].steps;
+        x.k = p[i].k;
         tiles_of(x, cfg);
     }
     int* order = reinterpret_cast<int*>(img + L.order);
     for (int i = 0; i < n; ++i) order[i] = i;
     std::sort(order, order + n, [&](int a, int b) {
-        return d[a].steps != d[b].steps ? d[a].steps > d[b].steps : a < b;
+        return d[a].passes != d[b].passes ? d[a].passes > d[b].passes : a < b;
     });
     long long* tilepre = reinterpret_cast<long long*>(img + L.tilepre);
     tilepre[0] = 0;
@@ -395,7 +482,7 @@ cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t
     round[0] = 0;
     int active = n;
     for (int s = 0; s < max_steps; ++s) {
-        while (active > 0 && d[order[active - 1]].steps <= s) --active;
+        while (active > 0 && d[order[active - 1]].passes <= s) --active;
         round[s + 1] = round[s] + tilepre[active];
     }
     BatchHeader* h = reinterpret_cast<BatchHeader*>(img);
@@ -412,14 +499,18 @@ cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t
     if (e != cudaSuccess) return e;
     e = cudaStreamSynchronize(stream);  // the staging image is reused by the next call
     if (e != cudaSuccess) return e;
-    return batch_launch(ws, n, err, stream);
+    return batch_launch(ws, n, err, stream, cfg);
 }
 
-cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream) {
+cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream, int cfg) {
     cudaError_t e = cudaMemsetAsync(ws, 0, counter_bytes(n), stream);
     if (e != cudaSuccess) return e;
-    const int grid = sm_count() * blocks_per_sm_cached();
-    batch_kernel<<<grid, kThreads, 0, stream>>>(static_cast<unsigned char*>(ws), n, err);
+    unsigned char* w = static_cast<unsigned char*>(ws);
+    if (cfg >= kBatchTiles) {
+        batch_kernel<2><<<sm_count() * blocks_per_sm_cached<2>(), kThreads, 0, stream>>>(w, n, err);
+    } else {
+        batch_kernel<3><<<sm_count() * blocks_per_sm_cached<3>(), kThreads, 0, stream>>>(w, n, err);
+    }
     return cudaGetLastError();
 }
 

@@ -74,7 +74,9 @@ long long batch_workspace_bytes(const ph3_problem* p, int n);
 cudaError_t batch_prepare(const ph3_problem* p, int n, void* ws, long long ws_bytes,
                           cudaStream_t stream, long long* total_items, int cfg);
 int batch_configs(const char** names, int max);
-cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream);
+// cfg: the tuning table's batch configuration (>= 3: the two-blocks-per-SM kernel); the tile
+// geometry comes from the plan the workspace holds
+cudaError_t batch_launch(void* ws, int n, int* err, cudaStream_t stream, int cfg);
 long long batch_static_capacity();
 cudaError_t batch_run_static(const ph3_problem* p, int n, int* err, cudaStream_t stream,
                              long long* need_bytes, int cfg);

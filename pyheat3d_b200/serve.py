@@ -199,7 +199,7 @@ class GpuExecutor:
             c0, c1 = s.req.coefficients()
             d.c0, d.c1 = float(np.float32(c0)), float(np.float32(c1))
             d.steps = int(c)
-            d.reserved = 0
+            d.k = 1
         addr = ctypes.addressof(descs)
         need = int(self.lib.ph3_batch_workspace_bytes(addr, n))
         # the library's fixed workspace belongs to the current device: make it this one

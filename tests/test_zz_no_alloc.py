@@ -62,7 +62,7 @@ def test_static_batch_rejects_plans_beyond_its_array():
     d = descs[0]
     d.a, d.b, d.src = a.data_ptr(), b.data_ptr(), None
     d.dims, d.nz, d.ny, d.nx = 2, 1, 8, 8
-    d.bc, d.storage, d.c0, d.c1, d.steps, d.reserved = 1, 0, 0.5, 0.125, 400000, 0
+    d.bc, d.storage, d.c0, d.c1, d.steps, d.k = 1, 0, 0.5, 0.125, 400000, 1
     lib = _lib.lib()
     rc = lib.ph3_batch_run_static(ctypes.addressof(descs), 1, None)
     assert rc == 1
