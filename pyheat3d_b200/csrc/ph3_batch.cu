@@ -38,6 +38,7 @@
 #include "ph3_internal.h"
 #include "ph3_march.cuh"
 #include "ph3_tb2d.cuh"
+#include "ph3_tile3d.cuh"
 
 namespace ph3 {
 
@@ -86,59 +87,96 @@ static_assert(T2Cfg<float, 1, 4, 2>::OX == tb_strip_width<float, 2>() &&
 
 // Compiled tile configurations (the tuning table's batch family): rows per warp and planes per
 // 3D tile, rows per iteration and rows per 2D tile. The plan records which one it was built for.
+// S3: 3D tiles are the block-wide shared-memory plane tiles of ph3_tile3d.cuh (64 x 32 columns)
+// instead of one lean march per warp (32 columns x 8 R rows).
 template <int CFG> struct BCfg;
-template <> struct BCfg<0> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128; };
-template <> struct BCfg<1> { static constexpr int R = 2, ZCH = 16, RB2 = 4, YCH = 64; };
-template <> struct BCfg<2> { static constexpr int R = 8, ZCH = 64, RB2 = 8, YCH = 256; };
-// Configurations 3 .. 5 are 0 .. 2 with the kernel compiled for two blocks per SM instead of
-// three (128 registers per thread instead of 80: the tile bodies no longer spill).
-constexpr int kBatchTiles = 3;
-constexpr int kBatchCfgs = 6;
-const char* kBatchNames[kBatchCfgs] = {"R4_Z32_Y128",    "R2_Z16_Y64",    "R8_Z64_Y256",
-                                       "R4_Z32_Y128_B2", "R2_Z16_Y64_B2", "R8_Z64_Y256_B2"};
+template <> struct BCfg<0> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128; static constexpr bool S3 = false; };
+template <> struct BCfg<1> { static constexpr int R = 2, ZCH = 16, RB2 = 4, YCH = 64; static constexpr bool S3 = false; };
+template <> struct BCfg<2> { static constexpr int R = 8, ZCH = 64, RB2 = 8, YCH = 256; static constexpr bool S3 = false; };
+template <> struct BCfg<3> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128; static constexpr bool S3 = true; };
+template <> struct BCfg<4> { static constexpr int R = 4, ZCH = 16, RB2 = 4, YCH = 64; static constexpr bool S3 = true; };
+template <> struct BCfg<5> { static constexpr int R = 4, ZCH = 64, RB2 = 8, YCH = 256; static constexpr bool S3 = true; };
+// Configurations kBatchTiles .. 2 kBatchTiles - 1 are the same tile sets with the kernel compiled
+// for two blocks per SM instead of three (128 registers per thread instead of 80: the tile bodies
+// no longer spill).
+constexpr int kBatchTiles = 6;
+constexpr int kBatchCfgs = 2 * kBatchTiles;
+const char* kBatchNames[kBatchCfgs] = {
+    "R4_Z32_Y128",    "R2_Z16_Y64",    "R8_Z64_Y256",    "S64x32_Z32_Y128",    "S64x32_Z16_Y64",
+    "S64x32_Z64_Y256", "R4_Z32_Y128_B2", "R2_Z16_Y64_B2", "R8_Z64_Y256_B2", "S64x32_Z32_Y128_B2",
+    "S64x32_Z16_Y64_B2", "S64x32_Z64_Y256_B2"};
 
-struct Geo { int R, ZCH, YCH; };
+// shared-memory plane ring of the 3D tiles of tile sets with S3 (one per block)
+__shared__ __align__(16) float g_tile_sm[Tile3::SMEM / 4];
+
+struct Geo { int R, ZCH, YCH; bool S3; };
+template <int CFG> Geo geo_t() { return {BCfg<CFG>::R, BCfg<CFG>::ZCH, BCfg<CFG>::YCH, BCfg<CFG>::S3}; }
 Geo geo_of(int cfg) {
     switch (cfg) {
-        case 1: return {BCfg<1>::R, BCfg<1>::ZCH, BCfg<1>::YCH};
-        case 2: return {BCfg<2>::R, BCfg<2>::ZCH, BCfg<2>::YCH};
-        default: return {BCfg<0>::R, BCfg<0>::ZCH, BCfg<0>::YCH};
+        case 1: return geo_t<1>();
+        case 2: return geo_t<2>();
+        case 3: return geo_t<3>();
+        case 4: return geo_t<4>();
+        case 5: return geo_t<5>();
+        default: return geo_t<0>();
     }
 }
 constexpr int kThreads = 32 * kW;
+static_assert(Tile3::W == kW, "3D plane tiles take the whole block");
 
 __host__ __device__ __forceinline__ long long counter_bytes(int n) {
     return ((16LL + 8LL * n + 255) / 256) * 256;
 }
 long long align256(long long x) { return ((x + 255) / 256) * 256; }
 
-// Not inlined: each (storage, boundary, configuration) tile body keeps its own register
-// allocation instead of the kernel carrying the union of all of them.
-template <typename T, bool PER, int CFG>
-__device__ __noinline__ void run_tile(const BatchDesc& d, int s, int t) {
-    using C = BCfg<CFG>;
+// Not inlined: each tile body (storage, boundary, tile shape, with or without a Jacobi source)
+// keeps its own register allocation instead of the kernel carrying the union of all of them.
+template <typename T, bool PER, int ZCH, bool SRC>
+__device__ __noinline__ void run_plane_tile3(const BatchDesc& d, int s, int t) {
+    const T* src = static_cast<const T*>((s & 1) ? d.b : d.a);
+    T* dst = static_cast<T*>((s & 1) ? d.a : d.b);
+    const int tx = t % d.ntx, ty = (t / d.ntx) % d.nty, tz = t / (d.ntx * d.nty);
+    const int z0 = tz * ZCH, z1 = min(z0 + ZCH, d.nz);
+    tile3d_item<T, PER, SRC, true>(src, dst, SRC ? d.src : nullptr, d.nz, d.ny, d.nx, d.c0, d.c1,
+                                   tx, ty, z0, z1, g_tile_sm);
+}
+
+template <typename T, bool PER, int R, int ZCH, bool SRC>
+__device__ __noinline__ void run_lean_tile3(const BatchDesc& d, int s, int t) {
     const T* src = static_cast<const T*>((s & 1) ? d.b : d.a);
     T* dst = static_cast<T*>((s & 1) ? d.a : d.b);
     const int w = threadIdx.x >> 5;
-    // problems without a Jacobi source take tiles compiled without it
-    if (d.dims == 3) {
-        const int tx = t % d.ntx, ty = (t / d.ntx) % d.nty, tz = t / (d.ntx * d.nty);
-        const int z0 = tz * C::ZCH, z1 = min(z0 + C::ZCH, d.nz), y0 = (ty * kW + w) * C::R;
-        if (d.src != nullptr)
-            lite3d_item<T, PER, C::R, true, true>(src, dst, d.src, d.nz, d.ny, d.nx, d.c0, d.c1,
-                                                  tx, y0, z0, z1);
-        else
-            lite3d_item<T, PER, C::R, true, false>(src, dst, nullptr, d.nz, d.ny, d.nx, d.c0,
-                                                   d.c1, tx, y0, z0, z1);
+    const int tx = t % d.ntx, ty = (t / d.ntx) % d.nty, tz = t / (d.ntx * d.nty);
+    const int z0 = tz * ZCH, z1 = min(z0 + ZCH, d.nz), y0 = (ty * kW + w) * R;
+    lite3d_item<T, PER, R, true, SRC>(src, dst, SRC ? d.src : nullptr, d.nz, d.ny, d.nx, d.c0,
+                                      d.c1, tx, y0, z0, z1);
+}
+
+template <typename T, bool PER, int RB2, int YCH, bool SRC>
+__device__ __noinline__ void run_lean_tile2(const BatchDesc& d, int s, int t) {
+    const T* src = static_cast<const T*>((s & 1) ? d.b : d.a);
+    T* dst = static_cast<T*>((s & 1) ? d.a : d.b);
+    const int w = threadIdx.x >> 5;
+    const int tx = t % d.ntx, ty = t / d.ntx;
+    const int y0 = ty * YCH, y1 = min(y0 + YCH, d.ny);
+    lite2d_item<T, PER, RB2, true, SRC>(src, dst, SRC ? d.src : nullptr, d.ny, d.nx, d.c0, d.c1,
+                                        tx * kW + w, y0, y1);
+}
+
+// problems without a Jacobi source take tiles compiled without it
+template <typename T, bool PER, int CFG>
+__device__ __forceinline__ void run_tile(const BatchDesc& d, int s, int t) {
+    using C = BCfg<CFG>;
+    const bool src = d.src != nullptr;
+    if (d.dims == 3 && C::S3) {
+        if (src) run_plane_tile3<T, PER, C::ZCH, true>(d, s, t);
+        else run_plane_tile3<T, PER, C::ZCH, false>(d, s, t);
+    } else if (d.dims == 3) {
+        if (src) run_lean_tile3<T, PER, C::R, C::ZCH, true>(d, s, t);
+        else run_lean_tile3<T, PER, C::R, C::ZCH, false>(d, s, t);
     } else {
-        const int tx = t % d.ntx, ty = t / d.ntx;
-        const int y0 = ty * C::YCH, y1 = min(y0 + C::YCH, d.ny);
-        if (d.src != nullptr)
-            lite2d_item<T, PER, C::RB2, true, true>(src, dst, d.src, d.ny, d.nx, d.c0, d.c1,
-                                                    tx * kW + w, y0, y1);
-        else
-            lite2d_item<T, PER, C::RB2, true, false>(src, dst, nullptr, d.ny, d.nx, d.c0, d.c1,
-                                                     tx * kW + w, y0, y1);
+        if (src) run_lean_tile2<T, PER, C::RB2, C::YCH, true>(d, s, t);
+        else run_lean_tile2<T, PER, C::RB2, C::YCH, false>(d, s, t);
     }
 }
 
@@ -249,6 +287,9 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
         switch (cfg) {
             case 1: run_any<1>(d, s, t); break;
             case 2: run_any<2>(d, s, t); break;
+            case 3: run_any<3>(d, s, t); break;
+            case 4: run_any<4>(d, s, t); break;
+            case 5: run_any<5>(d, s, t); break;
             default: run_any<0>(d, s, t); break;
         }
         __syncthreads();
@@ -295,7 +336,11 @@ void tiles_of(BatchDesc& d, int cfg) {
         d.ntiles = d.ntx * d.nty;
         return;
     }
-    if (d.dims == 3) {
+    if (d.dims == 3 && g.S3) {
+        d.ntx = cdiv(d.nx, Tile3::OX);
+        d.nty = cdiv(d.ny, Tile3::OY);
+        d.ntz = cdiv(d.nz, g.ZCH);
+    } else if (d.dims == 3) {
         d.ntx = cdiv(d.nx, 32);
         d.nty = cdiv(d.ny, kW * g.R);
         d.ntz = cdiv(d.nz, g.ZCH);

@@ -13,6 +13,7 @@
 #include "ph3_common.cuh"
 #include "ph3_internal.h"
 #include "ph3_march.cuh"
+#include "ph3_tile3d.cuh"
 
 namespace ph3 {
 
@@ -107,6 +108,16 @@ lite3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restric
     const int z0 = zb + blockIdx.z * zch;
     lite3d_item<T, PER, R, false, SRC>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x,
                                        (blockIdx.y * W + w) * R, z0, min(z0 + zch, ze));
+}
+
+template <typename T, bool PER, bool SRC>
+__global__ void __launch_bounds__(32 * Tile3::W)
+tile3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
+              int ny, int nx, float c0, float c1, int zch) {
+    __shared__ __align__(16) float sm[Tile3::SMEM / 4];
+    const int z0 = blockIdx.z * zch;
+    tile3d_item<T, PER, SRC, false>(u, o, b, nz, ny, nx, c0, c1, blockIdx.x, blockIdx.y, z0,
+                                    min(z0 + zch, nz), sm);
 }
 
 template <typename T, bool PER, int R, int W>
@@ -215,6 +226,21 @@ static cudaError_t march_k1_t(const Launch& L) {
         cfg = 0;
     }
     if (L.ze > 0) cfg = 0;  // z ranges: the lean march or the lane-vector march above
+    if (L.dims == 3 && cfg == 7) {
+        // block-wide shared-memory plane tiles, 64 x 32 columns
+        const long long tiles = 1LL * cdiv(L.nx, Tile3::OX) * cdiv(L.ny, Tile3::OY);
+        const int zch = L.chunk > 0 ? L.chunk : default_chunk(L.nz, tiles, 16, 2 * target);
+        dim3 grd(cdiv(L.nx, Tile3::OX), cdiv(L.ny, Tile3::OY), cdiv(L.nz, zch));
+        if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
+        if (int64_t(L.nx) * L.ny >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
+        if (L.src != nullptr)
+            tile3d_kernel<T, PER, true><<<grd, 32 * Tile3::W, 0, L.stream>>>(
+                u, o, L.src, L.nz, L.ny, L.nx, L.c0, L.c1, zch);
+        else
+            tile3d_kernel<T, PER, false><<<grd, 32 * Tile3::W, 0, L.stream>>>(
+                u, o, nullptr, L.nz, L.ny, L.nx, L.c0, L.c1, zch);
+        return cudaGetLastError();
+    }
     if (cfg == 0) {
         if (L.dims == 2) {
             constexpr int W = 4, RB = 4;
@@ -313,13 +339,15 @@ cudaError_t launch_tb(const Launch& L) {
 // 2D: 0 lean one-column-per-lane march, 1 float-window vector march, 2 / 3 / 4 raw-row vector
 // march with 4 / 8 / 6 rows per step (shapes without whole 16-byte rows fall back to 1). 3D: 0 lean,
 // 1 vector march, 2 / 3 any-alignment lane vectors with 4 / 2 rows per warp, 4 / 5 / 6 row boxes
-// by 1D tensor copies into per-warp rings (rows per warp, ring stages: 2/3, 2/4, 4/3).
+// by 1D tensor copies into per-warp rings (rows per warp, ring stages: 2/3, 2/4, 4/3), 7 block-wide
+// shared-memory plane tiles of 64 x 32 columns.
 int march_configs(int dims, const char** names, int max) {
     static const char* k2[] = {"lane1_W4_RB4", "V16B_W4_RB4", "raw16B_W4_RB4", "raw16B_W4_RB8",
                                "raw16B_W4_RB6"};
     static const char* k3[] = {"lane1_R4_W4", "V16B_R2_W8", "V4any_R4_W4", "V4any_R2_W4",
-                               "ring1d_R2_W4_S3", "ring1d_R2_W4_S4", "ring1d_R4_W4_S3"};
-    const int n = dims == 2 ? 5 : 7;
+                               "ring1d_R2_W4_S3", "ring1d_R2_W4_S4", "ring1d_R4_W4_S3",
+                               "smem_tile_64x32"};
+    const int n = dims == 2 ? 5 : 8;
     for (int i = 0; i < n && names != nullptr && i < max; ++i) names[i] = dims == 2 ? k2[i] : k3[i];
     return n;
 }

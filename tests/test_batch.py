@@ -77,10 +77,10 @@ def test_graph_replay_and_plain_steppers_agree():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("cfg", [0, 1])
+@pytest.mark.parametrize("cfg", [0, 1, 3, 10])
 def test_long_plan_with_few_tiles_per_step(cfg):
     """Long dependency chains (7000 and 3001 steps of grids that are one or two tiles each)
-    beside a short problem stay bit-exact, for two tile configurations."""
+    beside a short problem stay bit-exact, for four tile configurations."""
     from pyheat3d_b200 import _lib, heat_stencil, tune
     from pyheat3d_b200.batch import Batch, Problem
 
@@ -139,12 +139,13 @@ def _tb_mix(seed: int):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("cfg", [0, 2, 3, 5])
+@pytest.mark.parametrize("cfg", [0, 2, 3, 5, 6, 9])
 def test_temporal_blocking_problems_match_oracle_and_tb_steppers(cfg):
     """Per-problem k: a 2D problem with k = 2 or 4 advances by steps // k passes of k fused steps
     and steps % k single steps, rounded to its storage type once per pass — bit-identical to the
-    oracle's per-pass rounding and to the single-grid tb<k> stepper, in four batch kernel
-    configurations (tile sets compiled for three and for two blocks per SM)."""
+    oracle's per-pass rounding and to the single-grid tb<k> stepper, in six batch kernel
+    configurations (lean and shared-memory plane tile sets, compiled for three and for two blocks
+    per SM)."""
     from pyheat3d_b200 import _lib, tune
     from pyheat3d_b200.batch import Batch
     from pyheat3d_b200.registry import make_stepper

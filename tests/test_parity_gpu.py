@@ -273,8 +273,11 @@ def test_every_compiled_config(storage, bc):
     # 0..3 (nx = 261) or 0 / 2 (nx = 258): every access width of the lane-vector march
     u3b = rng.random((7, 10, 261), dtype=np.float32)
     u3c = rng.random((6, 9, 258), dtype=np.float32)
+    # several 64 x 32 plane tiles in x and y, partial at both ends
+    u3d = rng.random((11, 70, 133), dtype=np.float32)
     marches = [(2, u2, st2, "b200/ymarch" + suf), (3, u3, st, "b200/zmarch" + suf),
-               (3, u3b, st, "b200/zmarch" + suf), (3, u3c, st, "b200/zmarch" + suf)]
+               (3, u3b, st, "b200/zmarch" + suf), (3, u3c, st, "b200/zmarch" + suf),
+               (3, u3d, st, "b200/zmarch" + suf)]
     b3 = rng.random(u0.shape, dtype=np.float32) * np.float32(1e-2)
     b2 = rng.random(u2.shape, dtype=np.float32) * np.float32(1e-2)
     try:
