@@ -555,10 +555,12 @@ def bench_batching(torch, nprob: int = 512) -> dict:
     import ctypes
 
     from oracle import run_reference
-    from pyheat3d_b200 import _lib
+    from pyheat3d_b200 import _lib, tune
     from pyheat3d_b200.batch import Batch, synthetic_batch
 
-    probs = synthetic_batch(nprob, seed=0)
+    # 2D problems take the tuned temporal-block depth (k fused steps per pass); the plain path
+    # below runs each grid with the same depth, so results must agree bit for bit
+    probs = tune.with_batch_k(synthetic_batch(nprob, seed=0))
     batch = Batch(probs)
     upd = batch.updates
     g = batch.graph(with_reset=True)
@@ -582,8 +584,10 @@ def bench_batching(torch, nprob: int = 512) -> dict:
         st = torch.cuda.current_stream().cuda_stream
         for i, _ in enumerate(probs):
             d = batch.descs[i]
-            _lib.check(L.ph3_advance(d.dims, d.nz, d.ny, d.nx, d.storage, d.bc, d.c0, d.c1, 1,
-                                     1, d.a, d.b, d.src, d.steps, st, ctypes.byref(ib)))
+            variant = _lib.VARIANT["tb"] if d.k > 1 else _lib.VARIANT["march"]
+            _lib.check(L.ph3_advance(d.dims, d.nz, d.ny, d.nx, d.storage, d.bc, d.c0, d.c1,
+                                     variant, max(d.k, 1), d.a, d.b, d.src, d.steps, st,
+                                     ctypes.byref(ib)))
 
     batch.reset()
     torch.cuda.synchronize()
@@ -605,9 +609,14 @@ def bench_batching(torch, nprob: int = 512) -> dict:
                                 p.stencil.bc, p.steps)
             worst = max(worst, float(np.abs(outs[i] - ref).max() / np.abs(ref).max()))
         errs[st_name] = worst
+    cfg, chunk = ctypes.c_int(-1), ctypes.c_int(0)
+    _lib.check(L.ph3_tune_get(_lib.KERNEL["batch"], 3, 0, 1, ctypes.byref(cfg),
+                              ctypes.byref(chunk)))
+    tiles = L.ph3_tune_name(_lib.KERNEL["batch"], 3, 1, max(cfg.value, 0)).decode()
+    k2d = tune.batch_k2d()
     del batch, g
     torch.cuda.empty_cache()
-    return {"problems": len(probs), "updates": upd,
+    return {"problems": len(probs), "updates": upd, "tiles": tiles, "k_2d": k2d,
             "batched_s": round(batched, 4), "batched_solves_per_s": round(len(probs) / batched, 2),
             "batched_glups": round(upd / batched / 1e9, 2),
             "plain_s": round(plain_s, 4), "plain_solves_per_s": round(len(probs) / plain_s, 2),

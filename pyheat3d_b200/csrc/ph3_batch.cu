@@ -93,8 +93,8 @@ template <int CFG> struct BCfg;
 template <> struct BCfg<0> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128; static constexpr bool S3 = false; };
 template <> struct BCfg<1> { static constexpr int R = 2, ZCH = 16, RB2 = 4, YCH = 64; static constexpr bool S3 = false; };
 template <> struct BCfg<2> { static constexpr int R = 8, ZCH = 64, RB2 = 8, YCH = 256; static constexpr bool S3 = false; };
-template <> struct BCfg<3> { static constexpr int R = 4, ZCH = 32, RB2 = 4, YCH = 128; static constexpr bool S3 = true; };
-template <> struct BCfg<4> { static constexpr int R = 4, ZCH = 16, RB2 = 4, YCH = 64; static constexpr bool S3 = true; };
+template <> struct BCfg<3> { static constexpr int R = 4, ZCH = 256, RB2 = 8, YCH = 256; static constexpr bool S3 = true; };
+template <> struct BCfg<4> { static constexpr int R = 4, ZCH = 128, RB2 = 8, YCH = 256; static constexpr bool S3 = true; };
 template <> struct BCfg<5> { static constexpr int R = 4, ZCH = 64, RB2 = 8, YCH = 256; static constexpr bool S3 = true; };
 // Configurations kBatchTiles .. 2 kBatchTiles - 1 are the same tile sets with the kernel compiled
 // for two blocks per SM instead of three (128 registers per thread instead of 80: the tile bodies
@@ -102,9 +102,9 @@ template <> struct BCfg<5> { static constexpr int R = 4, ZCH = 64, RB2 = 8, YCH 
 constexpr int kBatchTiles = 6;
 constexpr int kBatchCfgs = 2 * kBatchTiles;
 const char* kBatchNames[kBatchCfgs] = {
-    "R4_Z32_Y128",    "R2_Z16_Y64",    "R8_Z64_Y256",    "S64x32_Z32_Y128",    "S64x32_Z16_Y64",
-    "S64x32_Z64_Y256", "R4_Z32_Y128_B2", "R2_Z16_Y64_B2", "R8_Z64_Y256_B2", "S64x32_Z32_Y128_B2",
-    "S64x32_Z16_Y64_B2", "S64x32_Z64_Y256_B2"};
+    "R4_Z32_Y128",    "R2_Z16_Y64",    "R8_Z64_Y256",    "S64x32_Z256_Y256",   "S64x32_Z128_Y256",
+    "S64x32_Z64_Y256", "R4_Z32_Y128_B2", "R2_Z16_Y64_B2", "R8_Z64_Y256_B2", "S64x32_Z256_Y256_B2",
+    "S64x32_Z128_Y256_B2", "S64x32_Z64_Y256_B2"};
 
 // shared-memory plane ring of the 3D tiles of tile sets with S3 (one per block)
 __shared__ __align__(16) float g_tile_sm[Tile3::SMEM / 4];

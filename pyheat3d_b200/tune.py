@@ -149,6 +149,21 @@ def configure_batch(lib=None) -> None:
         (lib or _lib.lib()).ph3_tune_set(_lib.KERNEL["batch"], 3, 0, 1, int(e["cfg"]), 0)
 
 
+def batch_k2d() -> int:
+    """Temporal-block depth the active table picked for the 2D problems of a batch (1: none)."""
+    t = active_table()
+    e = t.entries.get(_key("batch", 3, "float32", 1, "large")) if t is not None else None
+    return int(e.get("k2d", 1)) if e is not None else 1
+
+
+def with_batch_k(problems: list) -> list:
+    """The problems with the table's 2D temporal-block depth set on every 2D problem."""
+    import dataclasses
+
+    k = batch_k2d()
+    return [dataclasses.replace(p, k=k) if p.u0.ndim == 2 else p for p in problems]
+
+
 # ------------------------------------------------------------------------------------------
 # measurement
 # ------------------------------------------------------------------------------------------
@@ -230,36 +245,45 @@ def sweep_family(table: Table, kernel: str, dims: int, storage: str, k: int, n: 
 
 
 def sweep_batch(table: Table, quick: bool = False, verbose: bool = True) -> dict:
-    """Time the batch tile configurations on a scaled problem mix; record the winner."""
+    """Time every batch tile configuration with each 2D temporal-block depth (1, 2, 4) on a
+    problem mix of the batching workload's distribution (another seed; quick: a scaled-down mix);
+    record the fastest pair."""
+    import dataclasses
+
     import torch
 
     from .batch import Batch, synthetic_batch
 
     lib = _lib.lib()
     kid = _lib.KERNEL["batch"]
-    probs = synthetic_batch(64 if quick else 128, seed=1, n2d=(64, 1024 if quick else 2048),
-                            n3d=(32, 128 if quick else 256), steps=(20, 100 if quick else 400))
+    if quick:
+        base = synthetic_batch(64, seed=1, n2d=(64, 1024), n3d=(32, 128), steps=(20, 100))
+    else:
+        base = synthetic_batch(256, seed=1)
     best = None
     prev = active_table()
     use(None)
     try:
-        for cfg in range(lib.ph3_tune_count(kid, 3, 1)):
-            _lib.check(lib.ph3_tune_set(kid, 3, 0, 1, cfg, 0))
-            b = Batch(probs)
-            b.run()
-            torch.cuda.synchronize()
-            b.reset()
-            t0 = time.perf_counter()
-            b.run()
-            torch.cuda.synchronize()
-            dt = time.perf_counter() - t0
-            g = b.updates / dt / 1e9
-            name = lib.ph3_tune_name(kid, 3, 1, cfg).decode()
-            if verbose:
-                print(f"batch  {name:22s} {g:9.1f} GLUPS ({dt:.3f} s)", flush=True)
-            if best is None or g > best["glups"]:
-                best = {"cfg": cfg, "cfg_name": name, "chunk": 0, "glups": round(g, 2)}
-            del b
+        for k2d in (1, 2, 4):
+            probs = [dataclasses.replace(p, k=k2d) if p.u0.ndim == 2 else p for p in base]
+            for cfg in range(lib.ph3_tune_count(kid, 3, 1)):
+                _lib.check(lib.ph3_tune_set(kid, 3, 0, 1, cfg, 0))
+                b = Batch(probs)
+                b.run()
+                torch.cuda.synchronize()
+                b.reset()
+                t0 = time.perf_counter()
+                b.run()
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
+                g = b.updates / dt / 1e9
+                name = lib.ph3_tune_name(kid, 3, 1, cfg).decode()
+                if verbose:
+                    print(f"batch  {name:22s} k2d={k2d} {g:9.1f} GLUPS ({dt:.3f} s)", flush=True)
+                if best is None or g > best["glups"]:
+                    best = {"cfg": cfg, "cfg_name": name, "chunk": 0, "k2d": k2d,
+                            "glups": round(g, 2)}
+                del b
     finally:
         lib.ph3_tune_set(kid, 3, 0, 1, -1, 0)
         use(prev)
