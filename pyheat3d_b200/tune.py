@@ -259,7 +259,7 @@ def sweep_batch(table: Table, quick: bool = False, verbose: bool = True) -> dict
     if quick:
         base = synthetic_batch(64, seed=1, n2d=(64, 1024), n3d=(32, 128), steps=(20, 100))
     else:
-        base = synthetic_batch(256, seed=1)
+        base = synthetic_batch(512, seed=1)
     best = None
     prev = active_table()
     use(None)
