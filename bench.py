@@ -69,6 +69,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-batch", action="store_true", help="skip the batching measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--no-precision", action="store_true", help="skip the precision measurement")
+    ap.add_argument("--no-small", action="store_true",
+                    help="skip the 128^3 Dirichlet case (GPU and NumPy GLUPS, oracle error)")
     ap.add_argument("--zslab", default="auto", choices=("auto", "on", "off"),
                     help="z-slab split measurement: auto runs it on one GPU only (halos by "
                          "local copies); on also runs it across ranks (NCCL halo exchange)")
@@ -461,7 +463,8 @@ def run_b200(a: argparse.Namespace) -> None:
         extra["zslab"] = bench_zslab(torch, ws, rank, min(T, 200), value / ws)
         torch.cuda.empty_cache()
     if ws == 1:
-        for name, flag, fn in (("precision", a.no_precision,
+        for name, flag, fn in (("dirichlet_128cubed", a.no_small, lambda: bench_small(torch)),
+                               ("precision", a.no_precision,
                                 lambda: bench_precision(torch, a.precision_n)),
                                ("batching", a.no_batch,
                                 lambda: bench_batching(torch, a.batch_problems)),
@@ -677,6 +680,51 @@ def bench_serving(torch, seconds: float) -> dict:
                     "alone); both servers stop at the end of the stream; p50/p99 count the "
                     "unfinished requests by their age at that moment (censored, lower bounds); "
                     "Jacobi stops at relative residual <= tol or at max_sweeps"}
+
+
+def bench_small(torch) -> dict:
+    """The reference's CPU-runnable case: 3D 128^3 fp32 with Dirichlet walls (zero boundary
+    layer), r = 0.15, uniform [0, 1) from seed 0, 100 steps. GPU GLUPS of the tuned single-grid
+    path (``b200/auto``, CUDA events, field resident) beside the NumPy GLUPS of the oracle on one
+    host thread (pyheat3d's numpy/slicing backend runs one update per call the same way), and the
+    relative error of the GPU result against the oracle (stated bound 1e-6)."""
+    from oracle import reference_step
+    from pyheat3d_b200 import heat_stencil
+    from pyheat3d_b200.registry import make_stepper
+
+    n, steps = 128, 100
+    u0 = np.random.default_rng(0).random((n, n, n), dtype=np.float32)
+    u0[0] = u0[-1] = 0
+    u0[:, 0] = u0[:, -1] = 0
+    u0[:, :, 0] = u0[:, :, -1] = 0
+    st = heat_stencil(3, 0.15, "dirichlet")
+    cells = (n - 2) ** 3
+    s = make_stepper("b200/auto", u0, st)
+    s.step(steps)  # warm-up
+    s.synchronize()
+    best = None
+    for _ in range(5):
+        s.set_state(u0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        s.step(steps)
+        b.record()
+        b.synchronize()
+        t = a.elapsed_time(b) * 1e-3
+        best = t if best is None else min(best, t)
+    got = s.get()
+    s.close()
+    ref = u0.copy()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ref = reference_step(ref, st.c0, st.c1, "dirichlet")
+    cpu_s = time.perf_counter() - t0
+    err = float(np.abs(got.astype(np.float64) - ref).max() / np.abs(ref).max())
+    return {"grid": [n, n, n], "bc": "dirichlet", "r": 0.15, "steps": steps,
+            "units": "interior site updates", "gpu_glups": round(cells * steps / best / 1e9, 2),
+            "gpu_ms": round(best * 1e3, 3), "numpy_glups_1thread": round(cells * steps / cpu_s / 1e9, 4),
+            "rel_err_vs_oracle": err, "bitwise_equal": bool(np.array_equal(got, ref)),
+            "tolerance": 1e-6}
 
 
 def bench_precision(torch, n: int = 256) -> dict:
