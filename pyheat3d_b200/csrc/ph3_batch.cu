@@ -122,6 +122,7 @@ Geo geo_of(int cfg) {
     }
 }
 constexpr int kThreads = 32 * kW;
+constexpr int kSmemTilePre = 1024;  // tile prefix sums kept in shared memory (n < 1024)
 static_assert(Tile3::W == kW, "3D plane tiles take the whole block");
 
 __host__ __device__ __forceinline__ long long counter_bytes(int n) {
@@ -256,6 +257,14 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
     const long long total = hd->total_items;
     const int max_steps = hd->max_steps;
     const int cfg = hd->cfg % kBatchTiles;
+    // the tile prefix sums of short problem lists live in shared memory for the item decode
+    __shared__ long long s_tilepre[kSmemTilePre];
+    const bool tp_shared = n + 1 <= kSmemTilePre;
+    if (tp_shared)
+        for (int i = threadIdx.x; i <= n; i += blockDim.x) s_tilepre[i] = tilepre[i];
+    __syncthreads();
+    const long long* tp = tp_shared ? s_tilepre : tilepre;
+    int s_prev = 0;  // thread 0: round of its previous item (a block's items only increase)
 
     for (;;) {
         if (threadIdx.x == 0) {
@@ -263,13 +272,16 @@ batch_kernel(unsigned char* __restrict__ ws, int n, int* err) {
             if (item >= total || *reinterpret_cast<volatile int*>(abort_flag) != 0) {
                 item = -1;
             } else {
-                const int s = int(upper_bound_i64(round_off, max_steps + 1, item)) - 1;
+                int s = s_prev;  // round_off[s] <= item; most items stay in the same round
+                if (round_off[s + 1] <= item)
+                    s += int(upper_bound_i64(round_off + s, max_steps + 1 - s, item)) - 1;
+                s_prev = s;
                 const long long j = item - round_off[s];
-                const int q = int(upper_bound_i64(tilepre, n + 1, j)) - 1;
+                const int q = int(upper_bound_i64(tp, n + 1, j)) - 1;
                 const int p = order[q];
                 s_p = p;
                 s_s = s;
-                s_t = int(j - tilepre[q]);
+                s_t = int(j - tp[q]);
                 const unsigned long long need =
                     static_cast<unsigned long long>(s) * static_cast<unsigned long long>(desc[p].ntiles);
                 if (!wait_u64_geq(&done[p], need, kSpinLimit, err, abort_flag)) {
