@@ -24,6 +24,8 @@
 
 namespace ph3 {
 
+template <bool B> struct BoolTag { static constexpr bool value = B; };
+
 struct Tile3 {
     static constexpr int R = 4;                      // rows per warp
     static constexpr int W = 8;                      // warps per block
@@ -92,68 +94,102 @@ __device__ __forceinline__ void tile3d_item(const T* __restrict__ u, T* __restri
         float2 v[R];  // (column lane, column lane + 32) of each own row
         float h;
     };
-    auto load = [&](int z, Plane& p) {
-        const T* pl = u + int64_t(PER ? wrap_near(z, nz) : z) * P;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            p.v[r] = make_float2(ldx1<CG>(pl + roff[r] + cx[0]), ldx1<CG>(pl + roff[r] + cx[1]));
-        p.h = has_h ? ldx1<CG>(pl + hoff) : 0.f;
-    };
-    auto put = [&](const Plane& p, float* slot, bool halo) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            slot[own0 + r * SX] = p.v[r].x;
-            slot[own0 + r * SX + 32] = p.v[r].y;
-        }
-        if (halo && has_h) slot[hs] = p.h;
-    };
-    // plane p lives in slot (p - zlo + 1) mod 4
-    auto slot = [&](int p) { return sm + ((p - zlo + 1) & (C::SLOTS - 1)) * C::PLANE; };
+    // A tile whose own sites are all stored, with rows and columns that do not wrap (FULL):
+    // row r of this warp starts nx elements after row r-1 and column lane + 32 is 32 elements
+    // after column lane, so loads and stores walk one pointer with constant offsets and no
+    // per-site predicates. Other tiles take per-site offsets and store masks.
+    bool full;
+    if constexpr (PER) full = x0 + C::OX <= nx && y0 + C::OY <= ny;
+    else full = x0 >= 1 && x0 + C::OX <= nx - 1 && y0 >= 1 && y0 + C::OY <= ny - 1;
+    const int base0 = roff[0] + cx[0];
 
-    const float2 c0v = make_float2(c0, c0), c1v = make_float2(c1, c1);
-    Plane A, B;
-    load(zlo - 1, A);
-    load(zlo, B);
-    put(A, slot(zlo - 1), false);  // lower neighbours of the first plane: own sites only
-    put(B, slot(zlo), true);
-    load(zlo + 1, A);
-
-    // plane z: abv holds plane z+1 (stored now when another plane follows), pre takes z+2
-    auto step = [&](int z, const Plane& abv, Plane& pre) -> bool {
-        const bool more = z + 1 < zhi;
-        if (more) {
-            put(abv, slot(z + 1), true);
-            load(z + 2, pre);
-        }
-        __syncthreads();
-        const float* cur = slot(z) + own0;
-        const float* prv = slot(z - 1) + own0;
-        T* opl = o + int64_t(z) * P;
-        float2 ym = make_float2(cur[-SX], cur[32 - SX]);  // row y-1 of the warp's first row
-        float2 ctr = make_float2(cur[0], cur[32]);
+    auto run = [&](auto full_tag) {
+        constexpr bool FULL = decltype(full_tag)::value;
+        auto load = [&](int z, Plane& p) {
+            const T* pl = u + int64_t(PER ? wrap_near(z, nz) : z) * P;
+            if constexpr (FULL) {
+                const T* q = pl + base0;
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const float* row = cur + r * SX;
-            const float2 yp = make_float2(row[SX], row[32 + SX]);
-            const float2 xm = make_float2(row[-1], row[31]);
-            const float2 xp = make_float2(row[1], row[33]);
-            const float2 zm = make_float2(prv[r * SX], prv[r * SX + 32]);
-            float2 v = upd3_x2(c0v, c1v, ctr, xm, xp, ym, yp, zm, abv.v[r]);
-            if constexpr (SRC) {
-                const float* bp = b + int64_t(z) * P + roff[r];
-                v = add2(v, make_float2(__ldg(bp + cx[0]), __ldg(bp + cx[1])));
+                for (int r = 0; r < R; ++r, q += nx)
+                    p.v[r] = make_float2(ldx1<CG>(q), ldx1<CG>(q + 32));
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    p.v[r] = make_float2(ldx1<CG>(pl + roff[r] + cx[0]),
+                                         ldx1<CG>(pl + roff[r] + cx[1]));
             }
-            if ((store >> (2 * r)) & 1u) opl[roff[r] + cx[0]] = from_f<T>(v.x);
-            if ((store >> (2 * r + 1)) & 1u) opl[roff[r] + cx[1]] = from_f<T>(v.y);
-            ym = ctr;
-            ctr = yp;
+            p.h = has_h ? ldx1<CG>(pl + hoff) : 0.f;
+        };
+        auto put = [&](const Plane& p, float* slot, bool halo) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                slot[own0 + r * SX] = p.v[r].x;
+                slot[own0 + r * SX + 32] = p.v[r].y;
+            }
+            if (halo && has_h) slot[hs] = p.h;
+        };
+        // plane p lives in slot (p - zlo + 1) mod 4
+        auto slot = [&](int p) { return sm + ((p - zlo + 1) & (C::SLOTS - 1)) * C::PLANE; };
+
+        const float2 c0v = make_float2(c0, c0), c1v = make_float2(c1, c1);
+        Plane A, B;
+        load(zlo - 1, A);
+        load(zlo, B);
+        put(A, slot(zlo - 1), false);  // lower neighbours of the first plane: own sites only
+        put(B, slot(zlo), true);
+        load(zlo + 1, A);
+
+        // plane z: abv holds plane z+1 (stored now when another plane follows), pre takes z+2
+        auto step = [&](int z, const Plane& abv, Plane& pre) -> bool {
+            const bool more = z + 1 < zhi;
+            if (more) {
+                put(abv, slot(z + 1), true);
+                load(z + 2, pre);
+            }
+            __syncthreads();
+            const float* cur = slot(z) + own0;
+            const float* prv = slot(z - 1) + own0;
+            T* opl = o + int64_t(z) * P;
+            T* wq = opl + base0;  // FULL: the warp's row r, column lane
+            const float* bq = SRC ? b + int64_t(z) * P + base0 : nullptr;
+            float2 ym = make_float2(cur[-SX], cur[32 - SX]);  // row y-1 of the warp's first row
+            float2 ctr = make_float2(cur[0], cur[32]);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const float* row = cur + r * SX;
+                const float2 yp = make_float2(row[SX], row[32 + SX]);
+                const float2 xm = make_float2(row[-1], row[31]);
+                const float2 xp = make_float2(row[1], row[33]);
+                const float2 zm = make_float2(prv[r * SX], prv[r * SX + 32]);
+                float2 v = upd3_x2(c0v, c1v, ctr, xm, xp, ym, yp, zm, abv.v[r]);
+                if constexpr (FULL) {
+                    if constexpr (SRC) {
+                        v = add2(v, make_float2(__ldg(bq), __ldg(bq + 32)));
+                        bq += nx;
+                    }
+                    wq[0] = from_f<T>(v.x);
+                    wq[32] = from_f<T>(v.y);
+                    wq += nx;
+                } else {
+                    if constexpr (SRC) {
+                        const float* bp = b + int64_t(z) * P + roff[r];
+                        v = add2(v, make_float2(__ldg(bp + cx[0]), __ldg(bp + cx[1])));
+                    }
+                    if ((store >> (2 * r)) & 1u) opl[roff[r] + cx[0]] = from_f<T>(v.x);
+                    if ((store >> (2 * r + 1)) & 1u) opl[roff[r] + cx[1]] = from_f<T>(v.y);
+                }
+                ym = ctr;
+                ctr = yp;
+            }
+            return more;
+        };
+        for (int z = zlo;;) {
+            if (!step(z++, A, B)) break;
+            if (!step(z++, B, A)) break;
         }
-        return more;
     };
-    for (int z = zlo;;) {
-        if (!step(z++, A, B)) break;
-        if (!step(z++, B, A)) break;
-    }
+    if (full) run(BoolTag<true>{});
+    else run(BoolTag<false>{});
 }
 
 }  // namespace ph3
