@@ -21,24 +21,30 @@ namespace ph3 {
 // naive: one lattice site per thread; every operand through L1/L2. The site's offset is formed
 // once; the neighbours are signed deltas from it (+-1, +-nx, +-nx*ny), replaced by the wrapped
 // delta only on the periodic boundary, so a site costs seven loads, the update and one store.
+// Index arithmetic is in I: 32-bit whenever the field has fewer than 2^31 elements (one 32-bit
+// offset per site, one wide address per load), 64-bit otherwise. The block shape is a
+// compile-time constant.
 // ------------------------------------------------------------------------------------------
-template <typename T, bool PER, bool SRC>
+constexpr int kNaive2X = 32, kNaive2Y = 8;
+constexpr int kNaive3X = 32, kNaive3Y = 4, kNaive3Z = 2;
+
+template <typename T, bool PER, bool SRC, typename I>
 __global__ void __launch_bounds__(256)
 naive2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int ny,
                int nx, float c0, float c1) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.x * kNaive2X + threadIdx.x;
+    const int j = blockIdx.y * kNaive2Y + threadIdx.y;
     if (i >= nx || j >= ny) return;
     if constexpr (!PER) {
         if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1) return;
     }
-    const int64_t c = int64_t(j) * nx + i;
-    int64_t xm = -1, xp = 1, ym = -int64_t(nx), yp = nx;
+    const I c = I(j) * nx + i;
+    I xm = -1, xp = 1, ym = -I(nx), yp = nx;
     if constexpr (PER) {
-        if (i == 0) xm = nx - 1;
-        if (i == nx - 1) xp = 1 - nx;
-        if (j == 0) ym = int64_t(ny - 1) * nx;
-        if (j == ny - 1) yp = -int64_t(ny - 1) * nx;
+        xm = i == 0 ? I(nx - 1) : xm;
+        xp = i == nx - 1 ? I(1 - nx) : xp;
+        ym = j == 0 ? I(ny - 1) * nx : ym;
+        yp = j == ny - 1 ? -I(ny - 1) * nx : yp;
     }
     const T* p = u + c;
     float v = upd2(c0, c1, ldg1(p), ldg1(p + xm), ldg1(p + xp), ldg1(p + ym), ldg1(p + yp));
@@ -46,27 +52,27 @@ naive2d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restri
     o[c] = from_f<T>(v);
 }
 
-template <typename T, bool PER, bool SRC>
+template <typename T, bool PER, bool SRC, typename I>
 __global__ void __launch_bounds__(256)
 naive3d_kernel(const T* __restrict__ u, T* __restrict__ o, const float* __restrict__ b, int nz,
                int ny, int nx, float c0, float c1) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z * blockDim.z + threadIdx.z;
+    const int i = blockIdx.x * kNaive3X + threadIdx.x;
+    const int j = blockIdx.y * kNaive3Y + threadIdx.y;
+    const int k = blockIdx.z * kNaive3Z + threadIdx.z;
     if (i >= nx || j >= ny || k >= nz) return;
     if constexpr (!PER) {
         if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1 || k == 0 || k == nz - 1) return;
     }
-    const int64_t P = int64_t(nx) * ny;
-    const int64_t c = int64_t(k) * P + int64_t(j) * nx + i;
-    int64_t xm = -1, xp = 1, ym = -int64_t(nx), yp = nx, zm = -P, zp = P;
+    const I P = I(nx) * ny;
+    const I c = I(k) * P + I(j) * nx + i;
+    I xm = -1, xp = 1, ym = -I(nx), yp = nx, zm = -P, zp = P;
     if constexpr (PER) {
-        if (i == 0) xm = nx - 1;
-        if (i == nx - 1) xp = 1 - nx;
-        if (j == 0) ym = P - nx;
-        if (j == ny - 1) yp = nx - P;
-        if (k == 0) zm = (nz - 1) * P;
-        if (k == nz - 1) zp = -(nz - 1) * P;
+        xm = i == 0 ? I(nx - 1) : xm;
+        xp = i == nx - 1 ? I(1 - nx) : xp;
+        ym = j == 0 ? P - nx : ym;
+        yp = j == ny - 1 ? nx - P : yp;
+        zm = k == 0 ? I(nz - 1) * P : zm;
+        zp = k == nz - 1 ? -I(nz - 1) * P : zp;
     }
     const T* p = u + c;
     float v = upd3(c0, c1, ldg1(p), ldg1(p + xm), ldg1(p + xp), ldg1(p + ym), ldg1(p + yp),
@@ -157,30 +163,39 @@ int default_chunk(int n_march, long long tiles, int min_len, long long target_ct
     return std::min(std::max(len, 1), n_march);
 }
 
-template <typename T, bool PER>
-static cudaError_t naive_t(const Launch& L) {
+template <typename T, bool PER, typename I>
+static cudaError_t naive_launch(const Launch& L) {
     const T* u = static_cast<const T*>(L.u);
     T* o = static_cast<T*>(L.out);
     if (L.dims == 2) {
-        dim3 blk(32, 8), grd(cdiv(L.nx, 32), cdiv(L.ny, 8));
+        dim3 blk(kNaive2X, kNaive2Y), grd(cdiv(L.nx, kNaive2X), cdiv(L.ny, kNaive2Y));
         if (grd.y > 65535) return cudaErrorInvalidConfiguration;
         if (L.src != nullptr)
-            naive2d_kernel<T, PER, true><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.ny, L.nx, L.c0,
-                                                                    L.c1);
+            naive2d_kernel<T, PER, true, I><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.ny, L.nx,
+                                                                       L.c0, L.c1);
         else
-            naive2d_kernel<T, PER, false><<<grd, blk, 0, L.stream>>>(u, o, nullptr, L.ny, L.nx,
-                                                                     L.c0, L.c1);
+            naive2d_kernel<T, PER, false, I><<<grd, blk, 0, L.stream>>>(u, o, nullptr, L.ny, L.nx,
+                                                                        L.c0, L.c1);
     } else {
-        dim3 blk(32, 4, 2), grd(cdiv(L.nx, 32), cdiv(L.ny, 4), cdiv(L.nz, 2));
+        dim3 blk(kNaive3X, kNaive3Y, kNaive3Z);
+        dim3 grd(cdiv(L.nx, kNaive3X), cdiv(L.ny, kNaive3Y), cdiv(L.nz, kNaive3Z));
         if (grd.y > 65535 || grd.z > 65535) return cudaErrorInvalidConfiguration;
         if (L.src != nullptr)
-            naive3d_kernel<T, PER, true><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.nz, L.ny, L.nx,
-                                                                    L.c0, L.c1);
+            naive3d_kernel<T, PER, true, I><<<grd, blk, 0, L.stream>>>(u, o, L.src, L.nz, L.ny,
+                                                                       L.nx, L.c0, L.c1);
         else
-            naive3d_kernel<T, PER, false><<<grd, blk, 0, L.stream>>>(u, o, nullptr, L.nz, L.ny,
-                                                                     L.nx, L.c0, L.c1);
+            naive3d_kernel<T, PER, false, I><<<grd, blk, 0, L.stream>>>(u, o, nullptr, L.nz, L.ny,
+                                                                        L.nx, L.c0, L.c1);
     }
     return cudaGetLastError();
+}
+
+template <typename T, bool PER>
+static cudaError_t naive_t(const Launch& L) {
+    const long long n = 1LL * (L.dims == 2 ? 1 : L.nz) * L.ny * L.nx;
+    // 32-bit offsets when every offset and wrapped delta (|delta| < n) fits
+    if (n < (1LL << 31)) return naive_launch<T, PER, int>(L);
+    return naive_launch<T, PER, int64_t>(L);
 }
 
 template <typename T, bool PER, int V>
