@@ -972,9 +972,11 @@ cudaError_t zmarch_t_src(const Launch& L) {
         // one-wave z-slab schedule reads 2.5% less but leaves blocks idle and is slower)
         const long long plane_bytes = 1LL * L.nx * L.ny * sizeof(T);
         const long long cap = std::max(8LL, (64LL << 20) / std::max(1LL, 2 * plane_bytes));
-        // small grids: shorter chunks so that there are about three items per resident block
+        // small grids: shorter chunks so that there are about three items per resident block;
+        // down to two planes for grids of a few tiles (128^3: 3 planes, 64^3: 2), where the
+        // step time is one item's march through its chunk
         const long long fill = (1LL * g.nzi * tiles + 3 * resident - 1) / (3 * resident);
-        zch = int(std::max(8LL, std::min({cap, 32LL, fill})));
+        zch = int(std::max(2LL, std::min({cap, 32LL, fill})));
         zch = std::max(1, std::min(zch, g.nzi));
     }
     g.zch = zch;

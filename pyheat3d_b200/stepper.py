@@ -5,11 +5,17 @@ two device buffers hold the ping-pong pair, ``step(n)`` runs ``n // k`` fused pa
 ``n % k`` single steps and is asynchronous, ``get()`` returns a host float32 array. Differences:
 the buffers are torch CUDA tensors, the kernels are called through the ``libph3b200`` C ABI on
 torch's current stream, and a Jacobi source term is supported (``source=``).
+
+Small grids (fewer than ``GRAPH_CELLS`` sites) are bound by kernel launches, not by memory: a
+repeated ``step(n)`` of the same n from the same buffer replays a CUDA graph of that advance
+(captured on its second occurrence, after one plain run has set up every launch), with the same
+kernels and results. ``PH3_STEP_GRAPHS=0`` turns this off.
 """
 
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -32,6 +38,8 @@ class B200Stepper(Stepper):
     kind = "march"
     K = 1
     storage = "float32"
+    GRAPH_CELLS = 1 << 22  # grids below this size replay repeated advances as CUDA graphs
+    GRAPH_MIN_STEPS = 8
 
     def __init__(self, u0: np.ndarray, stencil, source: np.ndarray | None = None):
         super().__init__(u0, stencil, source)
@@ -75,21 +83,46 @@ class B200Stepper(Stepper):
                 _lib.BC[self.bc], self._k, ctypes.byref(tx), ctypes.byref(ty), ctypes.byref(ch)))
             self.tile.update({"tx": tx.value, "ty": ty.value, "zch": ch.value})
         self._in_b = ctypes.c_int(0)
+        self._graphs: dict = {}  # (n, start buffer) -> (CUDA graph, ends in the other buffer)
+        self._seen: set = set()  # (n, start buffer) advances run once plainly
+        self._use_graphs = (self.ncells < self.GRAPH_CELLS
+                            and os.environ.get("PH3_STEP_GRAPHS", "1") != "0")
 
     # -- stepping ------------------------------------------------------------------------
-    def step(self, n: int = 1) -> None:
-        if n < 0:
-            raise ValueError("n must be >= 0")
-        torch = _torch()
-        stream = torch.cuda.current_stream(self.device).cuda_stream
+    def _advance(self, n: int, stream: int) -> bool:
         src = self.src.data_ptr() if self.src is not None else None
-        configure(self.dims, self.storage, self._k, self.ncells, self._lib)
         _lib.check(self._lib.ph3_advance(
             self.dims, self._nz, self._ny, self._nx, _lib.STORAGE[self.storage],
             _lib.BC[self.bc], self._c0, self._c1, self._variant, self._k,
             self.a.data_ptr(), self.b.data_ptr(), src, int(n), stream,
             ctypes.byref(self._in_b)))
-        if self._in_b.value:
+        return bool(self._in_b.value)
+
+    def step(self, n: int = 1) -> None:
+        if n < 0:
+            raise ValueError("n must be >= 0")
+        torch = _torch()
+        cur = torch.cuda.current_stream(self.device)
+        configure(self.dims, self.storage, self._k, self.ncells, self._lib)
+        key = (int(n), self.a.data_ptr())
+        if self._use_graphs and n >= self.GRAPH_MIN_STEPS and not torch.cuda.is_current_stream_capturing():
+            g = self._graphs.get(key)
+            if g is None and key in self._seen:  # second occurrence: capture, then replay
+                side = torch.cuda.Stream(self.device)
+                side.wait_stream(cur)
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph, stream=side):
+                    swap = self._advance(n, side.cuda_stream)
+                cur.wait_stream(side)
+                g = self._graphs[key] = (graph, swap)
+            if g is not None:
+                g[0].replay()
+                if g[1]:
+                    self.a, self.b = self.b, self.a
+                self.steps_done += n
+                return
+            self._seen.add(key)
+        if self._advance(n, cur.cuda_stream):
             self.a, self.b = self.b, self.a
         self.steps_done += n
 
@@ -134,6 +167,7 @@ class B200Stepper(Stepper):
         _torch().cuda.synchronize(self.device)
 
     def close(self) -> None:
+        self._graphs.clear()
         self.a = self.b = self.src = None
 
 

@@ -283,7 +283,7 @@ def test_every_compiled_config(storage, bc):
     try:
         for fam, k, key in cases:
             for cfg in range(L.ph3_tune_count(K[fam], 3, k)):
-                for chunk in (0, 5):
+                for chunk in (0, 2, 5):
                     _lib.check(L.ph3_tune_set(K[fam], 3, S, k, cfg, chunk))
                     steps = 2 * k + 1
                     _assert_same(_run(key, u0, st, steps), _ref(key, u0, st, steps),
