@@ -49,7 +49,11 @@ __device__ __forceinline__ void tile3d_item(const T* __restrict__ u, T* __restri
     using C = Tile3;
     constexpr int R = C::R, SX = C::SX;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, t = threadIdx.x;
-    const int x0 = tx * C::OX, y0 = ty * C::OY;
+    // the last tile of a row or column of tiles ends at the grid's edge, overlapping its
+    // neighbour (the overlap is computed twice and stored twice with the same values), so every
+    // tile of a grid at least one tile wide lies inside the grid
+    const int x0 = nx >= C::OX ? min(tx * C::OX, nx - C::OX) : tx * C::OX;
+    const int y0 = ny >= C::OY ? min(ty * C::OY, ny - C::OY) : ty * C::OY;
     if constexpr (!PER) { zlo = max(zlo, 1); zhi = min(zhi, nz - 1); }
     if (zlo >= zhi) return;  // block-uniform
     const int64_t P = int64_t(nx) * ny;
@@ -61,6 +65,7 @@ __device__ __forceinline__ void tile3d_item(const T* __restrict__ u, T* __restri
     // own sites: rows y0 + 4w + r, columns x0 + lane + 32 j
     int roff[R], cx[2];
     uint32_t store = 0;  // bit 2r + j: site is stored (inside the grid, not a fixed boundary)
+    uint32_t fixm = 0;   // bit 2r + j: Dirichlet boundary site inside the grid (keeps its value)
 #pragma unroll
     for (int j = 0; j < 2; ++j) cx[j] = fx(x0 + lane + 32 * j, nx);
 #pragma unroll
@@ -71,7 +76,11 @@ __device__ __forceinline__ void tile3d_item(const T* __restrict__ u, T* __restri
         for (int j = 0; j < 2; ++j) {
             const int x = x0 + lane + 32 * j;
             bool ok = x < nx && y < ny;
-            if constexpr (!PER) ok = ok && x > 0 && x < nx - 1 && y > 0 && y < ny - 1;
+            if constexpr (!PER) {
+                if (ok && (x == 0 || x == nx - 1 || y == 0 || y == ny - 1))
+                    fixm |= 1u << (2 * r + j);
+                ok = ok && x > 0 && x < nx - 1 && y > 0 && y < ny - 1;
+            }
             if (ok) store |= 1u << (2 * r + j);
         }
     }
@@ -94,13 +103,12 @@ __device__ __forceinline__ void tile3d_item(const T* __restrict__ u, T* __restri
         float2 v[R];  // (column lane, column lane + 32) of each own row
         float h;
     };
-    // A tile whose own sites are all stored, with rows and columns that do not wrap (FULL):
-    // row r of this warp starts nx elements after row r-1 and column lane + 32 is 32 elements
-    // after column lane, so loads and stores walk one pointer with constant offsets and no
-    // per-site predicates. Other tiles take per-site offsets and store masks.
-    bool full;
-    if constexpr (PER) full = x0 + C::OX <= nx && y0 + C::OY <= ny;
-    else full = x0 >= 1 && x0 + C::OX <= nx - 1 && y0 >= 1 && y0 + C::OY <= ny - 1;
+    // A tile inside the grid (FULL: every tile of a grid at least 64 x 32): row r of this warp
+    // starts nx elements after row r-1 and column lane + 32 is 32 elements after column lane,
+    // so loads and stores walk one pointer with constant offsets, and every own site is stored;
+    // a Dirichlet boundary site stores its own unchanged value (the other buffer holds the same
+    // boundary values). Other tiles take per-site offsets and store masks.
+    const bool full = x0 + C::OX <= nx && y0 + C::OY <= ny;
     const int base0 = roff[0] + cx[0];
 
     auto run = [&](auto full_tag) {
@@ -166,6 +174,12 @@ __device__ __forceinline__ void tile3d_item(const T* __restrict__ u, T* __restri
                     if constexpr (SRC) {
                         v = add2(v, make_float2(__ldg(bq), __ldg(bq + 32)));
                         bq += nx;
+                    }
+                    if constexpr (!PER) {
+                        if (fixm != 0) {
+                            if ((fixm >> (2 * r)) & 1u) v.x = ctr.x;
+                            if ((fixm >> (2 * r + 1)) & 1u) v.y = ctr.y;
+                        }
                     }
                     wq[0] = from_f<T>(v.x);
                     wq[32] = from_f<T>(v.y);
