@@ -143,3 +143,17 @@ def test_2d_16384_16bit_periodic(case2, key):
     ref = threaded_emulated(u0, st.c0, st.c1, "periodic", n, var.storage, var.steps_per_pass,
                             threads=THREADS)
     _assert_same(_gpu(key, u0, st, n), ref, f"{key} 16384^2 periodic {n} steps")
+
+
+# ------------------------------------------------------------ unaligned rows, tuned defaults
+@pytest.mark.parametrize("n,bc,key", [(255, "periodic", "b200/zmarch"),
+                                      (255, "dirichlet", "b200/zmarch-bf16"),
+                                      (127, "periodic", "b200/zmarch-fp16")])
+def test_3d_unaligned_rows_tuned_defaults(n, bc, key):
+    """Rows without 16-byte vectors take the march family's tuned configuration (shared-memory
+    plane tiles with overlapped edge tiles from 255^3 up, the lean march below)."""
+    st = heat_stencil(3, 0.95 / 6, bc)
+    u0 = _field(3, n, bc)
+    var = VARIANTS[key]
+    ref = threaded_emulated(u0, st.c0, st.c1, bc, 5, var.storage, 1, threads=THREADS)
+    _assert_same(_gpu(key, u0, st, 5), ref, f"{key} {n}^3 {bc} 5 steps")
